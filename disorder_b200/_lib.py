@@ -1,0 +1,90 @@
+"""ctypes binding of libdisorder.so (the C ABI in include/disorder.h).
+
+The library is built in-tree by ``python -m disorder_b200.build``. There is no
+fallback: if the library or a CUDA device is missing, loading raises.
+"""
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdisorder.so")
+
+STATUS = {0: "OK", 1: "BAD_ARG", 2: "UNSUPPORTED_FIELD", 3: "OOM", 4: "CUDA_ERR", 5: "TIMEOUT",
+          6: "NONFINITE"}
+
+
+class DisorderError(RuntimeError):
+    """A libdisorder call returned a non-OK status (the MEX gateway maps the
+    same statuses to MATLAB errors with identifier disorder:<status>)."""
+
+    def __init__(self, status, msg):
+        self.status = status
+        super().__init__("disorder:%s %s" % (STATUS.get(status, status), msg))
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("N", C.c_int32 * 3), ("rG", C.POINTER(C.c_float) * 3), ("kG", C.POINTER(C.c_float) * 3),
+                ("cent", C.c_float * 3)]
+
+
+class SamplingDesc(C.Structure):
+    _fields_ = [("n_seg", C.c_int32), ("n_mot", C.c_int32), ("seg_offsets", C.POINTER(C.c_int64)),
+                ("ky", C.POINTER(C.c_int32)), ("kz", C.POINTER(C.c_int32))]
+
+
+VP = C.c_void_p
+FP = C.POINTER(C.c_float)
+DP = C.POINTER(C.c_double)
+I32 = C.c_int32
+
+# (name, restype, argtypes)
+SIGNATURES = [
+    ("disorder_ctx_create", C.c_int, [C.c_int, C.POINTER(VP)]),
+    ("disorder_ctx_destroy", C.c_int, [VP]),
+    ("disorder_last_error", C.c_char_p, [VP]),
+    ("disorder_ctx_set_stream", C.c_int, [VP, VP]),
+    ("disorder_ctx_get_stream", VP, [VP]),
+    ("disorder_synchronize", C.c_int, [VP]),
+    ("disorder_malloc", C.c_int, [VP, C.c_size_t, C.POINTER(VP)]),
+    ("disorder_free", C.c_int, [VP, VP]),
+    ("disorder_memcpy_h2d", C.c_int, [VP, VP, VP, C.c_size_t]),
+    ("disorder_memcpy_d2h", C.c_int, [VP, VP, VP, C.c_size_t]),
+    ("disorder_kernel_launches", C.c_int64, [VP]),
+    ("disorder_event_record", C.c_int, [VP, I32]),
+    ("disorder_event_elapsed", C.c_int, [VP, I32, I32, FP]),
+    ("disorder_plan_create", C.c_int, [VP, C.POINTER(GridDesc), C.POINTER(SamplingDesc), C.POINTER(VP)]),
+    ("disorder_plan_destroy", C.c_int, [VP]),
+    ("disorder_sinc_rigid_transform", C.c_int, [VP, VP, VP, I32, FP, I32, I32, I32, I32, VP]),
+    ("disorder_sinc_rigid_transform_gradient", C.c_int, [VP, VP, VP, FP, I32, VP, VP]),
+    ("disorder_encode", C.c_int, [VP, VP, VP, VP, I32, FP, VP]),
+    ("disorder_decode", C.c_int, [VP, VP, VP, VP, I32, FP, VP, VP, VP]),
+    ("disorder_encodedecode", C.c_int, [VP, VP, VP, VP, I32, FP, VP, VP]),
+    ("disorder_compute_energy", C.c_int, [VP, VP, VP, VP, VP, I32, FP, VP, VP, VP, DP]),
+    ("disorder_cg_solve", C.c_int, [VP, VP, VP, VP, I32, FP, VP, VP, VP, VP, VP, VP, VP, I32, I32, I32, C.c_double,
+                                    DP, C.POINTER(I32), C.POINTER(I32)]),
+    ("disorder_lm_step", C.c_int, [VP, VP, VP, VP, I32, VP, FP, FP, C.POINTER(C.c_uint8), C.c_float, FP, I32, I32,
+                                   DP, DP]),
+]
+
+_lib = None
+
+
+def load():
+    """Load libdisorder.so once and declare the signatures. Raises OSError if
+    the library was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libdisorder.so not built (run python -m disorder_b200.build): %s" % LIB_PATH)
+        lib = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    return [s[0] for s in SIGNATURES]

@@ -1,0 +1,479 @@
+// C ABI of libdisorder: contexts, workspaces, plans and the entry points
+// declared in include/disorder.h.
+#include <algorithm>
+#include <cstdarg>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "encoding.h"
+#include "internal.h"
+#include "solvers.h"
+
+int dis_set_error(disorder_ctx_s* ctx, int status, const char* fmt, ...) {
+  if (ctx) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(ctx->err, sizeof(ctx->err), fmt, ap);
+    va_end(ap);
+  }
+  return status;
+}
+
+static int grow(disorder_ctx_s* ctx, void** buf, size_t* cap, size_t bytes) {
+  if (bytes <= *cap && *buf) return DISORDER_OK;
+  if (*buf) {
+    DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    cudaFree(*buf);
+    *buf = nullptr;
+    *cap = 0;
+  }
+  const size_t want = std::max<size_t>(bytes + bytes / 8, 1 << 20);
+  cudaError_t e = cudaMalloc(buf, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *buf = nullptr;
+    return dis_set_error(ctx, DISORDER_OOM, "cudaMalloc of %zu bytes failed: %s", want, cudaGetErrorString(e));
+  }
+  *cap = want;
+  return DISORDER_OK;
+}
+
+int dis_workspace(disorder_ctx_s* ctx, size_t bytes, Workspace* ws) {
+  DIS_TRY(grow(ctx, &ctx->ws, &ctx->ws_bytes, bytes));
+  ws->base = (char*)ctx->ws;
+  ws->cap = ctx->ws_bytes;
+  ws->off = 0;
+  return DISORDER_OK;
+}
+
+int dis_workspace2(disorder_ctx_s* ctx, size_t bytes, Workspace* ws) {
+  DIS_TRY(grow(ctx, &ctx->ws2, &ctx->ws2_bytes, bytes));
+  ws->base = (char*)ctx->ws2;
+  ws->cap = ctx->ws2_bytes;
+  ws->off = 0;
+  return DISORDER_OK;
+}
+
+int dis_small(disorder_ctx_s* ctx, Workspace* ws) {
+  DIS_TRY(grow(ctx, &ctx->small, &ctx->small_bytes, 16u << 20));
+  ws->base = (char*)ctx->small;
+  ws->cap = ctx->small_bytes;
+  ws->off = 0;
+  return DISORDER_OK;
+}
+
+#define CTX_CHECK(ctx) \
+  if (!(ctx)) return DISORDER_BAD_ARG
+#define DEV_GUARD(ctx) DIS_CUDA_TRY(cudaSetDevice((ctx)->device))
+
+extern "C" {
+
+int disorder_ctx_create(int device, disorder_ctx* out) {
+  if (!out) return DISORDER_BAD_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return DISORDER_CUDA_ERR;
+  }
+  disorder_ctx_s* ctx = new disorder_ctx_s();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete ctx;
+    return DISORDER_CUDA_ERR;
+  }
+  cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  ctx->smem_optin = optin;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return DISORDER_CUDA_ERR;
+  }
+  ctx->own_stream = true;
+  *out = ctx;
+  return DISORDER_OK;
+}
+
+int disorder_ctx_destroy(disorder_ctx ctx) {
+  CTX_CHECK(ctx);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->ws2) cudaFree(ctx->ws2);
+  if (ctx->small) cudaFree(ctx->small);
+  for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return DISORDER_OK;
+}
+
+const char* disorder_last_error(disorder_ctx ctx) { return ctx ? ctx->err : "null context"; }
+
+int disorder_ctx_set_stream(disorder_ctx ctx, void* s) {
+  CTX_CHECK(ctx);
+  DEV_GUARD(ctx);
+  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  if (s) {
+    ctx->stream = (cudaStream_t)s;
+    ctx->own_stream = false;
+  } else {
+    DIS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->own_stream = true;
+  }
+  return DISORDER_OK;
+}
+
+void* disorder_ctx_get_stream(disorder_ctx ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int disorder_synchronize(disorder_ctx ctx) {
+  CTX_CHECK(ctx);
+  DEV_GUARD(ctx);
+  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return DISORDER_OK;
+}
+
+int disorder_malloc(disorder_ctx ctx, size_t bytes, void** dptr) {
+  CTX_CHECK(ctx);
+  if (!dptr) return dis_set_error(ctx, DISORDER_BAD_ARG, "malloc: null output");
+  DEV_GUARD(ctx);
+  cudaError_t e = cudaMalloc(dptr, std::max<size_t>(bytes, 1));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return dis_set_error(ctx, DISORDER_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  return DISORDER_OK;
+}
+
+int disorder_free(disorder_ctx ctx, void* dptr) {
+  CTX_CHECK(ctx);
+  DEV_GUARD(ctx);
+  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  DIS_CUDA_TRY(cudaFree(dptr));
+  return DISORDER_OK;
+}
+
+int disorder_memcpy_h2d(disorder_ctx ctx, void* dst, const void* src, size_t bytes) {
+  CTX_CHECK(ctx);
+  DEV_GUARD(ctx);
+  DIS_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return DISORDER_OK;
+}
+
+int disorder_memcpy_d2h(disorder_ctx ctx, void* dst, const void* src, size_t bytes) {
+  CTX_CHECK(ctx);
+  DEV_GUARD(ctx);
+  DIS_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return DISORDER_OK;
+}
+
+int64_t disorder_kernel_launches(disorder_ctx ctx) { return ctx ? ctx->launches : -1; }
+
+int disorder_event_record(disorder_ctx ctx, int32_t slot) {
+  CTX_CHECK(ctx);
+  if (slot < 0 || slot >= 16) return dis_set_error(ctx, DISORDER_BAD_ARG, "event slot %d", slot);
+  DEV_GUARD(ctx);
+  if (!ctx->ev[slot]) DIS_CUDA_TRY(cudaEventCreate(&ctx->ev[slot]));
+  DIS_CUDA_TRY(cudaEventRecord(ctx->ev[slot], ctx->stream));
+  return DISORDER_OK;
+}
+
+int disorder_event_elapsed(disorder_ctx ctx, int32_t a, int32_t b, float* ms) {
+  CTX_CHECK(ctx);
+  if (a < 0 || a >= 16 || b < 0 || b >= 16 || !ctx->ev[a] || !ctx->ev[b] || !ms)
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "event_elapsed: bad slots");
+  DEV_GUARD(ctx);
+  DIS_CUDA_TRY(cudaEventSynchronize(ctx->ev[b]));
+  DIS_CUDA_TRY(cudaEventElapsedTime(ms, ctx->ev[a], ctx->ev[b]));
+  return DISORDER_OK;
+}
+
+// ---------------------------------------------------------------- plans
+int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* g, const disorder_sampling_desc* smp,
+                         disorder_plan* out) {
+  CTX_CHECK(ctx);
+  if (!g || !smp || !out) return dis_set_error(ctx, DISORDER_BAD_ARG, "plan: null argument");
+  *out = nullptr;
+  DEV_GUARD(ctx);
+  disorder_plan_s* p = new disorder_plan_s();
+  p->ctx = ctx;
+  auto fail = [&](int st) {
+    disorder_plan_destroy(p);
+    return st;
+  };
+  for (int m = 0; m < 3; ++m) {
+    p->N[m] = g->N[m];
+    if (g->N[m] < 1 || g->N[m] > 1024) return fail(dis_set_error(ctx, DISORDER_BAD_ARG, "plan: N[%d]=%d out of range", m, g->N[m]));
+    if (!dis_make_fft_plan(g->N[m], &p->fft[m]))
+      return fail(dis_set_error(ctx, DISORDER_BAD_ARG,
+                                "plan: N[%d]=%d has a prime factor other than 2,3,5,7,11,13", m, g->N[m]));
+    if (!g->rG[m] || !g->kG[m]) return fail(dis_set_error(ctx, DISORDER_BAD_ARG, "plan: missing grid %d", m));
+    p->rG[m].assign(g->rG[m], g->rG[m] + g->N[m]);
+    p->kG[m].assign(g->kG[m], g->kG[m] + g->N[m]);
+    p->cent[m] = g->cent[m];
+  }
+  p->V = (long long)p->N[0] * p->N[1] * p->N[2];
+  for (int m = 0; m < 3; ++m) {
+    if (cudaMalloc(&p->d_kG[m], sizeof(float) * p->N[m]) != cudaSuccess ||
+        cudaMalloc(&p->d_rG[m], sizeof(float) * p->N[m]) != cudaSuccess)
+      return fail(dis_set_error(ctx, DISORDER_OOM, "plan: grid allocation"));
+    cudaMemcpy(p->d_kG[m], p->kG[m].data(), sizeof(float) * p->N[m], cudaMemcpyHostToDevice);
+    cudaMemcpy(p->d_rG[m], p->rG[m].data(), sizeof(float) * p->N[m], cudaMemcpyHostToDevice);
+  }
+  // sampling
+  if (smp->n_seg < 0 || smp->n_mot < 0 || smp->n_mot > smp->n_seg || !smp->seg_offsets)
+    return fail(dis_set_error(ctx, DISORDER_BAD_ARG, "plan: bad segment counts"));
+  p->n_seg = smp->n_seg;
+  p->n_mot = smp->n_mot;
+  p->seg_off.assign(smp->seg_offsets, smp->seg_offsets + smp->n_seg + 1);
+  if (p->seg_off[0] != 0) return fail(dis_set_error(ctx, DISORDER_BAD_ARG, "plan: seg_offsets[0] must be 0"));
+  for (int s = 0; s < p->n_seg; ++s)
+    if (p->seg_off[s + 1] < p->seg_off[s]) return fail(dis_set_error(ctx, DISORDER_BAD_ARG, "plan: seg_offsets decrease"));
+  const long long ns = p->seg_off[p->n_seg];
+  p->n_samples = ns;
+  if (ns > 0x7fffffffLL) return fail(dis_set_error(ctx, DISORDER_BAD_ARG, "plan: too many samples"));
+  const int N1 = p->N[0], N2 = p->N[1];
+  std::vector<int> segof(ns), rowptr((size_t)p->n_seg * (N1 + 1), 0), perm(ns);
+  for (int s = 0; s < p->n_seg; ++s) {
+    int* rp = rowptr.data() + (size_t)s * (N1 + 1);
+    for (long long i = p->seg_off[s]; i < p->seg_off[s + 1]; ++i) {
+      const int ky = smp->ky[i], kz = smp->kz[i];
+      if (ky < 0 || ky >= N1 || kz < 0 || kz >= N2)
+        return fail(dis_set_error(ctx, DISORDER_BAD_ARG, "plan: sample %lld row (%d,%d) outside %dx%d", i, ky, kz, N1, N2));
+      segof[i] = s;
+      rp[ky + 1]++;
+    }
+    for (int k = 0; k < N1; ++k) rp[k + 1] += rp[k];
+    std::vector<int> fill(rp, rp + N1);
+    for (long long i = p->seg_off[s]; i < p->seg_off[s + 1]; ++i) perm[p->seg_off[s] + fill[smp->ky[i]]++] = (int)i;
+    for (int k = 0; k <= N1; ++k) rp[k] += (int)p->seg_off[s];
+  }
+  auto up = [&](void** d, const void* h, size_t bytes) -> bool {
+    if (cudaMalloc(d, std::max<size_t>(bytes, 4)) != cudaSuccess) return false;
+    if (bytes) cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice);
+    return true;
+  };
+  if (!up((void**)&p->d_ky, smp->ky, sizeof(int) * ns) || !up((void**)&p->d_kz, smp->kz, sizeof(int) * ns) ||
+      !up((void**)&p->d_seg_of, segof.data(), sizeof(int) * ns) ||
+      !up((void**)&p->d_perm, perm.data(), sizeof(int) * ns) ||
+      !up((void**)&p->d_rowptr, rowptr.data(), sizeof(int) * rowptr.size()) ||
+      !up((void**)&p->d_seg_off, p->seg_off.data(), sizeof(long long) * p->seg_off.size()))
+    return fail(dis_set_error(ctx, DISORDER_OOM, "plan: sample table allocation"));
+  if (cudaGetLastError() != cudaSuccess) return fail(dis_set_error(ctx, DISORDER_CUDA_ERR, "plan: upload failed"));
+  *out = p;
+  return DISORDER_OK;
+}
+
+int disorder_plan_destroy(disorder_plan p) {
+  if (!p) return DISORDER_BAD_ARG;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(p->ctx->stream);
+  for (int m = 0; m < 3; ++m) {
+    cudaFree(p->d_kG[m]);
+    cudaFree(p->d_rG[m]);
+  }
+  cudaFree(p->d_ky);
+  cudaFree(p->d_kz);
+  cudaFree(p->d_seg_of);
+  cudaFree(p->d_perm);
+  cudaFree(p->d_rowptr);
+  cudaFree(p->d_seg_off);
+  delete p;
+  return DISORDER_OK;
+}
+
+#define PLAN_CHECK(ctx, plan)                                                        \
+  CTX_CHECK(ctx);                                                                    \
+  if (!(plan) || (plan)->ctx != (ctx)) return dis_set_error(ctx, DISORDER_BAD_ARG, "bad plan"); \
+  DEV_GUARD(ctx)
+
+static std::vector<int> all_segs(const disorder_plan_s* p) {
+  std::vector<int> v(p->n_seg);
+  std::iota(v.begin(), v.end(), 0);
+  return v;
+}
+
+// ---------------------------------------------------------------- transform
+int disorder_sinc_rigid_transform(disorder_ctx ctx, disorder_plan plan, const void* x, int32_t x_states,
+                                  const float* T, int32_t n_states, int32_t di, int32_t sumR, int32_t useFull,
+                                  void* out) {
+  PLAN_CHECK(ctx, plan);
+  if (!x || !T || !out || n_states < 1 || (x_states != 1 && x_states != n_states) || (di != 0 && di != 1) ||
+      useFull < -1 || useFull > 1)
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "sinc_rigid_transform: bad arguments");
+  const long long V = plan->V;
+  std::vector<SlotParams> prm;
+  dis_slot_params(T, n_states, nullptr, n_states, di, &prm);
+  const size_t tbytes = dis_table_bytes(plan, n_states, false);
+  const bool need_copy = (di == 0 && sumR);
+  Workspace ws;
+  DIS_TRY(dis_workspace(ctx, tbytes + (need_copy ? sizeof(float2) * V * n_states : 0) + (1 << 20), &ws));
+  Tables tb;
+  DIS_TRY(dis_build_tables(ctx, plan, prm, false, &ws, &tb));
+  const float2* xin = (const float2*)x;
+  if (di == 1) {
+    DIS_TRY(dis_forward_transform(ctx, plan, xin, x_states == 1 ? 0 : V, (float2*)out, tb, useFull, nullptr));
+    return DISORDER_OK;
+  }
+  float2* u = need_copy ? ws.take<float2>((size_t)V * n_states) : (float2*)out;
+  if (!u) return dis_set_error(ctx, DISORDER_OOM, "workspace");
+  if (x_states == 1 && n_states > 1) {
+    DIS_TRY(dis_broadcast(ctx, xin, V, n_states, u));
+  } else if ((const void*)u != x) {
+    DIS_CUDA_TRY(cudaMemcpyAsync(u, xin, sizeof(float2) * V * n_states, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  DIS_TRY(dis_inverse_transform(ctx, plan, u, tb, useFull, sumR ? (float2*)out : nullptr, 0.f));
+  return DISORDER_OK;
+}
+
+int disorder_sinc_rigid_transform_gradient(disorder_ctx ctx, disorder_plan plan, const void* x, const float* T,
+                                           int32_t n_states, void* G, void* xT) {
+  PLAN_CHECK(ctx, plan);
+  if (!x || !T || !G || n_states < 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "gradient: bad arguments");
+  const long long V = plan->V;
+  std::vector<SlotParams> prm;
+  dis_slot_params(T, n_states, nullptr, n_states, 1, &prm);
+  const size_t vols = (xT ? 4 : 5) * (size_t)n_states * V * sizeof(float2);
+  Workspace ws;
+  DIS_TRY(dis_workspace(ctx, vols + dis_table_bytes(plan, n_states, true) + (1 << 20), &ws));
+  Tables tb;
+  DIS_TRY(dis_build_tables(ctx, plan, prm, true, &ws, &tb));
+  float2* z = xT ? (float2*)xT : ws.take<float2>((size_t)n_states * V);
+  float2* yB = ws.take<float2>((size_t)2 * n_states * V);
+  float2* w1 = ws.take<float2>((size_t)n_states * V);
+  float2* w2 = ws.take<float2>((size_t)n_states * V);
+  if (!z || !yB || !w1 || !w2) return dis_set_error(ctx, DISORDER_OOM, "workspace");
+  return dis_gradient(ctx, plan, (const float2*)x, 0, tb, z, yB, w1, w2, (float2*)G);
+}
+
+// ---------------------------------------------------------------- encoding
+int disorder_encode(disorder_ctx ctx, disorder_plan plan, const void* x, const void* Sf, int32_t n_coils,
+                    const float* T, void* y) {
+  PLAN_CHECK(ctx, plan);
+  if (!x || !Sf || !y || n_coils < 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "encode: bad arguments");
+  EncodeSpec sp;
+  sp.x = (const float2*)x;
+  sp.Sf = (const float2*)Sf;
+  sp.C = n_coils;
+  sp.T = T;
+  sp.T_n = plan->n_mot;
+  sp.segs = all_segs(plan);
+  sp.n3_lo = 0;
+  sp.N3c = plan->N[2];
+  sp.y_ld = plan->n_samples;
+  sp.y_n3off = 0;
+  sp.y_N3 = plan->N[2];
+  return dis_encode_segments(ctx, plan, sp, (float2*)y, nullptr);
+}
+
+int disorder_decode(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf, int32_t n_coils,
+                    const float* T, const float* We, const float* Mb, void* x) {
+  PLAN_CHECK(ctx, plan);
+  if (!x || !Sf || !y || n_coils < 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "decode: bad arguments");
+  DecodeSpec sp;
+  sp.y = (const float2*)y;
+  sp.Sf = (const float2*)Sf;
+  sp.C = n_coils;
+  sp.T = T;
+  sp.T_n = plan->n_mot;
+  sp.segs = all_segs(plan);
+  sp.We = We;
+  sp.Mb = Mb;
+  return dis_decode_segments(ctx, plan, sp, (float2*)x);
+}
+
+int disorder_encodedecode(disorder_ctx ctx, disorder_plan plan, const void* x, const void* Sf, int32_t n_coils,
+                          const float* T, const float* We, void* out) {
+  PLAN_CHECK(ctx, plan);
+  if (!x || !Sf || !out || n_coils < 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "encodedecode: bad arguments");
+  const long long wm = (long long)plan->n_seg * plan->N[0] * plan->N[1];
+  Workspace ws;
+  DIS_TRY(dis_workspace2(ctx, sizeof(float) * wm + (1 << 16), &ws));
+  float* wmap = ws.take<float>(wm);
+  if (!wmap) return dis_set_error(ctx, DISORDER_OOM, "workspace");
+  DIS_TRY(dis_build_weight_map(ctx, plan, We, wmap, 1.f));
+  EncodeDecodeSpec sp;
+  sp.x = (const float2*)x;
+  sp.Sf = (const float2*)Sf;
+  sp.C = n_coils;
+  sp.T = T;
+  sp.T_n = plan->n_mot;
+  sp.segs = all_segs(plan);
+  sp.wmap = wmap;
+  return dis_encodedecode_segments(ctx, plan, sp, (float2*)out);
+}
+
+int disorder_compute_energy(disorder_ctx ctx, disorder_plan plan, const void* y, const void* x, const void* Sf,
+                            int32_t n_coils, const float* T, const float* Mb, const float* Mbe, const float* R_Ti,
+                            double* En) {
+  PLAN_CHECK(ctx, plan);
+  if (!x || !Sf || !y || !En || n_coils < 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "energy: bad arguments");
+  const long long ny = plan->n_samples * plan->N[2] * (long long)n_coils;
+  Workspace ws;
+  DIS_TRY(dis_workspace2(ctx, sizeof(float2) * ny + sizeof(float) * plan->N[2] + (1 << 16), &ws));
+  float2* rbuf = ws.take<float2>(ny);
+  float* roww = ws.take<float>(plan->N[2]);
+  if (!rbuf || !roww) return dis_set_error(ctx, DISORDER_OOM, "workspace");
+  const float* rw = nullptr;
+  if (Mb || Mbe) {
+    std::vector<float> a(plan->N[2], 1.f), b(plan->N[2], 1.f);
+    if (Mb) DIS_CUDA_TRY(cudaMemcpy(a.data(), Mb, sizeof(float) * plan->N[2], cudaMemcpyDeviceToHost));
+    if (Mbe) DIS_CUDA_TRY(cudaMemcpy(b.data(), Mbe, sizeof(float) * plan->N[2], cudaMemcpyDeviceToHost));
+    for (int i = 0; i < plan->N[2]; ++i) a[i] *= b[i];
+    DIS_CUDA_TRY(cudaMemcpy(roww, a.data(), sizeof(float) * plan->N[2], cudaMemcpyHostToDevice));
+    rw = roww;
+  }
+  return dis_energy(ctx, plan, (const float2*)y, (const float2*)x, (const float2*)Sf, n_coils, T, rw, R_Ti, rbuf, En);
+}
+
+// ---------------------------------------------------------------- solvers
+int disorder_cg_solve(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf, int32_t n_coils,
+                      const float* T, const float* We, const float* Mb, const float* Mbe, const float* P_Se,
+                      const float* C_Ma, const float* R_Ti, void* x_inout, int32_t x_init, int32_t nIt,
+                      int32_t tolType, double tol, double* En, int32_t* n_en, int32_t* nn) {
+  PLAN_CHECK(ctx, plan);
+  if (!y || !Sf || !x_inout || n_coils < 1 || nIt < 0 || !n_en || !nn)
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "cg_solve: bad arguments");
+  CGSpec s;
+  s.y = (const float2*)y;
+  s.Sf = (const float2*)Sf;
+  s.C = n_coils;
+  s.T = T;
+  s.We = We;
+  s.Mb = Mb;
+  s.Mbe = Mbe;
+  s.P_Se = P_Se;
+  s.C_Ma = C_Ma;
+  s.R_Ti = R_Ti;
+  int a = 0, b = 0;
+  const int st = dis_cg_solve(ctx, plan, s, (float2*)x_inout, x_init, nIt, tolType, tol, En, &a, &b);
+  *n_en = a;
+  *nn = b;
+  return st;
+}
+
+int disorder_lm_step(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf, int32_t n_coils,
+                     const void* x, float* T, float* w, uint8_t* cT, float winit, const float* tL, int32_t n3_lo,
+                     int32_t n3_hi, double* En, double* EnPrev) {
+  PLAN_CHECK(ctx, plan);
+  if (!y || !Sf || !x || !T || !w || !cT || !tL || n_coils < 1)
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "lm_step: bad arguments");
+  LMSpec s;
+  s.y = (const float2*)y;
+  s.Sf = (const float2*)Sf;
+  s.C = n_coils;
+  s.x = (const float2*)x;
+  s.winit = winit;
+  s.tL[0] = tL[0];
+  s.tL[1] = tL[1];
+  s.n3_lo = n3_lo;
+  s.n3_hi = n3_hi;
+  return dis_lm_step(ctx, plan, s, T, w, cT, En, EnPrev);
+}
+
+}  // extern "C"

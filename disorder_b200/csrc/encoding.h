@@ -1,0 +1,56 @@
+// Encoder driver specifications (internal).
+#pragma once
+#include <vector>
+
+#include "internal.h"
+
+struct EncodeSpec {
+  const float2* x = nullptr;   // one volume
+  const float2* Sf = nullptr;  // full-readout coil maps
+  int C = 0;
+  const float* T = nullptr;    // host, T_n x 6 parameter-major (NULL: no motion)
+  int T_n = 0;
+  std::vector<int> segs;       // segments to encode, motion segments first
+  int n3_lo = 0, N3c = 0;      // readout range processed
+  long long y_ld = 0;          // leading dim of y (total samples)
+  int y_n3off = 0, y_N3 = 0;   // readout offset/extent of y's layout
+};
+
+struct DecodeSpec {
+  const float2* y = nullptr;
+  const float2* Sf = nullptr;
+  int C = 0;
+  const float* T = nullptr;
+  int T_n = 0;
+  std::vector<int> segs;
+  const float* We = nullptr;
+  const float* Mb = nullptr;
+};
+
+struct EncodeDecodeSpec {
+  const float2* x = nullptr;
+  const float2* Sf = nullptr;
+  int C = 0;
+  const float* T = nullptr;
+  int T_n = 0;
+  std::vector<int> segs;
+  const float* wmap = nullptr;  // [seg][N2][N1] sample weights of each grid point
+};
+
+size_t dis_budget_bytes();
+bool dis_any_motion(const float* T, int n);
+size_t dis_table_bytes(const disorder_plan_s* plan, int ns, bool grad);
+int dis_chunk_slots(const disorder_plan_s* plan, int C, int N3c, size_t extra_per_slot, int n_total);
+int dis_upload_ints(disorder_ctx_s* ctx, Workspace* ws, const std::vector<int>& v, int** out);
+int dis_encode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const EncodeSpec& sp, float2* y,
+                        const float2* y_meas);
+int dis_encode_volumes(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* vols, const int* d_segs,
+                       int n, const float2* Sf, int C, int n3_lo, int N3c, float2* A, float2* y, long long y_ld,
+                       int y_n3off, int y_N3, const float2* y_meas);
+int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const DecodeSpec& sp, float2* out);
+int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const EncodeDecodeSpec& sp,
+                              float2* out);
+int dis_gradient(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* x, long long x_s,
+                 const Tables& tb, float2* z, float2* yB, float2* w1, float2* w2, float2* G);
+int dis_sum_slots(disorder_ctx_s* ctx, const float2* u, long long V, int n_slots, float2* out, float beta);
+int dis_broadcast(disorder_ctx_s* ctx, const float2* x, long long V, int n_slots, float2* out);

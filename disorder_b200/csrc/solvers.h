@@ -1,0 +1,35 @@
+// Solver specifications (internal).
+#pragma once
+#include "internal.h"
+
+struct CGSpec {
+  const float2* y = nullptr;
+  const float2* Sf = nullptr;
+  int C = 0;
+  const float* T = nullptr;  // host n_mot x 6 or NULL
+  const float* We = nullptr;
+  const float* Mb = nullptr;
+  const float* Mbe = nullptr;
+  const float* P_Se = nullptr;
+  const float* C_Ma = nullptr;
+  const float* R_Ti = nullptr;
+};
+
+struct LMSpec {
+  const float2* y = nullptr;
+  const float2* Sf = nullptr;
+  int C = 0;
+  const float2* x = nullptr;
+  float winit = 1e-3f;
+  float tL[2] = {0.f, 0.f};
+  int n3_lo = 0, n3_hi = 0;
+};
+
+int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec& s, float2* x, int x_init, int nIt,
+                 int tolType, double tol, double* En, int* n_en, int* nn);
+int dis_lm_step(disorder_ctx_s* ctx, const disorder_plan_s* plan, const LMSpec& s, float* T, float* w, uint8_t* cT,
+                double* En, double* EnPrev);
+int dis_energy(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* y, const float2* x, const float2* Sf,
+               int C, const float* T, const float* rowW, const float* R_Ti, float2* rbuf, double* En);
+int dis_ti_energy(disorder_ctx_s* ctx, const float2* x, const float* ti, long long n, double* out);
+int dis_weighted_norm(disorder_ctx_s* ctx, const float2* b, const float* w, long long n, double* out);

@@ -1,0 +1,159 @@
+// Phase factors of the sinc rigid transform
+// (Methods/precomputeFactorsSincRigidTransform.m:158-240, gr=1, sh=1).
+// Per-state scalars (wrapped angles, tan/sin/cos) are formed on the host in
+// double precision; the per-element factors exp(i*phase) are evaluated on the
+// device in double precision and rounded to single. The 1/N of the inverse
+// DFT of the pass that applies a factor is folded into that factor.
+#include <cmath>
+
+#include "internal.h"
+
+namespace {
+
+const int TR0[3] = {0, 2, 1};  // tr(1,:) of sincRigidTransform.m:33 (0-based)
+const int TR1[3] = {1, 0, 2};  // tr(2,:)
+
+double wrap_to_pi(double x) {  // Mapping Toolbox wrapToPi, from its definition
+  if (x < -M_PI || x > M_PI) {
+    const double y = x + M_PI;
+    double w = y - std::floor(y / (2 * M_PI)) * (2 * M_PI);
+    if (w == 0 && y > 0) w = 2 * M_PI;
+    return w - M_PI;
+  }
+  return x;
+}
+
+double wrap_to_pi_half(double x) {  // Methods/wrapToPiHalf.m:9-12
+  double m = x - std::floor(x / M_PI) * M_PI;
+  if (m > M_PI / 2) m -= M_PI;
+  return m;
+}
+
+// e2/e3 tables: [slot][r][k], phase = coef[slot] * fl(rG[r] * kG[k]); k along the pass axis.
+__global__ void shear_table_kernel(float2* __restrict__ tab, float2* __restrict__ gtab, int nk, int nr,
+                                   const float* __restrict__ kG, const float* __restrict__ rG,
+                                   const double* __restrict__ coef, const double* __restrict__ gcoef,
+                                   int gsign, double invn, int n_slots) {
+  const long long per = (long long)nk * nr;
+  const long long tot = per * n_slots;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+    const int slot = (int)(e / per);
+    const long long rem = e - slot * per;
+    const int r = (int)(rem / nk), k = (int)(rem - (long long)r * nk);
+    const float rk = __fmul_rn(rG[r], kG[k]);  // rkGrid is a single-precision product
+    double s, c;
+    sincos(coef[slot] * (double)rk, &s, &c);
+    const float2 v = make_float2((float)(c * invn), (float)(s * invn));
+    tab[e] = v;
+    if (gtab) {
+      // etg2 = i*g*rk*e2 (gsign=+1), etg3 = -i*g*rk*e3 (gsign=-1)
+      const double a = gsign * gcoef[slot] * (double)rk;
+      gtab[e] = make_float2((float)(-a * s * invn), (float)(a * c * invn));
+    }
+  }
+}
+
+__global__ void trans_table_kernel(float2* __restrict__ tab, int nk, const float* __restrict__ kG,
+                                   const double* __restrict__ t, int n_slots) {
+  const long long tot = (long long)nk * n_slots;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+    const int slot = (int)(e / nk), k = (int)(e - (long long)slot * nk);
+    double s, c;
+    sincos(t[slot] * (double)kG[k], &s, &c);
+    tab[e] = make_float2((float)c, (float)s);
+  }
+}
+
+}  // namespace
+
+void dis_slot_params(const float* T, int n_states, const int* slots, int n_slots, int di,
+                     std::vector<SlotParams>* out) {
+  out->resize(n_slots);
+  const double sd = (di == 1) ? -1.0 : 1.0;    // (-1)^di
+  const double sdm = (di == 1) ? 1.0 : -1.0;   // (-1)^(di-1)
+  for (int j = 0; j < n_slots; ++j) {
+    const int s = slots ? slots[j] : j;
+    SlotParams& p = (*out)[j];
+    for (int a = 0; a < 3; ++a) p.t[a] = sd * (double)T[a * n_states + s];
+    for (int m = 0; m < 3; ++m) {
+      double th = wrap_to_pi((double)T[(3 + m) * n_states + s]);
+      p.flip[m] = std::fabs(th) > M_PI / 2 ? 1 : 0;
+      th = wrap_to_pi_half(th);
+      const double t2 = std::tan(th / 2);
+      p.tau[m] = sdm * t2;
+      p.sig[m] = sd * std::sin(th);
+      p.g2[m] = (1 + t2 * t2) / 2;
+      p.g3[m] = std::cos(th);
+    }
+  }
+}
+
+int dis_build_tables(disorder_ctx_s* ctx, const disorder_plan_s* plan, const std::vector<SlotParams>& sp,
+                     bool with_grad, Workspace* ws, Tables* tb) {
+  const int ns = (int)sp.size();
+  tb->n_slots = ns;
+  if (ns == 0) return DISORDER_OK;
+  const int* N = plan->N;
+  // per-slot scalars: [what][m][slot]
+  std::vector<double> h(ns * 15);
+  for (int j = 0; j < ns; ++j)
+    for (int m = 0; m < 3; ++m) {
+      h[(0 * 3 + m) * ns + j] = sp[j].tau[m];
+      h[(1 * 3 + m) * ns + j] = sp[j].sig[m];
+      h[(2 * 3 + m) * ns + j] = sp[j].g2[m];
+      h[(3 * 3 + m) * ns + j] = sp[j].g3[m];
+      h[(4 * 3 + m) * ns + j] = sp[j].t[m];
+    }
+  double* d = ws->take<double>(h.size());
+  if (!d) return dis_set_error(ctx, DISORDER_OOM, "tables: workspace too small");
+  DIS_CUDA_TRY(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  const int blocks = 2 * ctx->sm_count;
+  for (int m = 0; m < 3; ++m) {
+    const int a1 = TR0[m], a2 = TR1[m];
+    tb->e2s[m] = (long long)N[a1] * N[a2];
+    tb->e3s[m] = (long long)N[a2] * N[a1];
+    tb->e2[m] = ws->take<float2>(tb->e2s[m] * ns);
+    tb->e3[m] = ws->take<float2>(tb->e3s[m] * ns);
+    if (with_grad) {
+      tb->g2[m] = ws->take<float2>(tb->e2s[m] * ns);
+      tb->g3[m] = ws->take<float2>(tb->e3s[m] * ns);
+    } else {
+      tb->g2[m] = tb->g3[m] = nullptr;
+    }
+    if (!tb->e2[m] || !tb->e3[m] || (with_grad && (!tb->g2[m] || !tb->g3[m])))
+      return dis_set_error(ctx, DISORDER_OOM, "tables: workspace too small");
+    // e2{m}: k along a1, r along a2
+    shear_table_kernel<<<blocks, 256, 0, ctx->stream>>>(tb->e2[m], tb->g2[m], N[a1], N[a2], plan->d_kG[a1],
+                                                        plan->d_rG[a2], d + (0 * 3 + m) * ns, d + (2 * 3 + m) * ns,
+                                                        +1, 1.0 / N[a1], ns);
+    // e3{m}: k along a2, r along a1
+    shear_table_kernel<<<blocks, 256, 0, ctx->stream>>>(tb->e3[m], tb->g3[m], N[a2], N[a1], plan->d_kG[a2],
+                                                        plan->d_rG[a1], d + (1 * 3 + m) * ns, d + (3 * 3 + m) * ns,
+                                                        -1, 1.0 / N[a2], ns);
+    dis_count(ctx, 2);
+  }
+  for (int a = 0; a < 3; ++a) {
+    tb->e1s[a] = N[a];
+    tb->e1[a] = ws->take<float2>((size_t)N[a] * ns);
+    if (!tb->e1[a]) return dis_set_error(ctx, DISORDER_OOM, "tables: workspace too small");
+    trans_table_kernel<<<blocks, 256, 0, ctx->stream>>>(tb->e1[a], N[a], plan->d_kG[a], d + (4 * 3 + a) * ns, ns);
+    dis_count(ctx);
+  }
+  for (int m = 0; m < 3; ++m) {
+    tb->flip_slots[m].clear();
+    for (int j = 0; j < ns; ++j)
+      if (sp[j].flip[m]) tb->flip_slots[m].push_back(j);
+    tb->any_flip[m] = !tb->flip_slots[m].empty();
+    tb->d_flip_slots[m] = nullptr;
+    if (tb->any_flip[m]) {
+      tb->d_flip_slots[m] = ws->take<int>(tb->flip_slots[m].size());
+      if (!tb->d_flip_slots[m]) return dis_set_error(ctx, DISORDER_OOM, "tables: workspace too small");
+      DIS_CUDA_TRY(cudaMemcpyAsync(tb->d_flip_slots[m], tb->flip_slots[m].data(),
+                                   tb->flip_slots[m].size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    }
+  }
+  // (pageable-source async copies are staged before they return, so the
+  // host vectors above may go out of scope)
+  DIS_CUDA_TRY(cudaGetLastError());
+  return DISORDER_OK;
+}

@@ -1,0 +1,159 @@
+/*
+ * libdisorder: B200-native (sm_100a) aligned-reconstruction hot path of
+ * DISORDER (motion-corrected 3-D MRI). C ABI: plain pointers and sizes, no
+ * framework types.
+ *
+ * Conventions (all follow the reference MATLAB code, column-major):
+ *  - complex data are interleaved single precision (re, im) pairs;
+ *  - a volume x is N1 x N2 x N3 with dims 1-2 the phase encodes (ky, kz) and
+ *    dim 3 the readout; element (n1,n2,n3) is at n1 + N1*(n2 + N2*n3);
+ *  - coil sensitivities Sf are N1 x N2 x N3 x C (coil slowest);
+ *  - motion states are the slowest dim of a batch of volumes (dim 5);
+ *  - samples y are Ns x 1 x N3 x C (sample fastest, then readout, then coil),
+ *    grouped by segment as in Methods/buildHarmonicSampling.m;
+ *  - rigid transforms T are n_states x 6, parameter-major (T[p*n + s]), the
+ *    reference's [1 1 1 1 NS 6] array: translations t1..t3 in voxels of the
+ *    full-resolution grid, then rotations r1..r3 in radians;
+ *  - "device" pointers are CUDA device memory of the context's device;
+ *    "host" pointers are ordinary host memory.
+ * Every entry point returns a disorder_status; disorder_last_error() gives
+ * the message of the last failure on a context. Calls are stream-ordered on
+ * the context's stream and return after the work is enqueued unless noted;
+ * entry points with host outputs synchronise the stream.
+ */
+#ifndef DISORDER_H
+#define DISORDER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DISORDER_OK = 0,
+  DISORDER_BAD_ARG = 1,
+  DISORDER_UNSUPPORTED_FIELD = 2,
+  DISORDER_OOM = 3,
+  DISORDER_CUDA_ERR = 4,
+  DISORDER_TIMEOUT = 5,
+  DISORDER_NONFINITE = 6
+} disorder_status;
+
+typedef struct disorder_ctx_s* disorder_ctx;
+typedef struct disorder_plan_s* disorder_plan;
+
+/* ---- context, stream and memory (replaces MATLAB gpuArray/gather,
+ *      Methods/fftGPU.m:27-31 device selection; the MEX handle layer) ---- */
+int disorder_ctx_create(int device, disorder_ctx* out);
+int disorder_ctx_destroy(disorder_ctx ctx);
+const char* disorder_last_error(disorder_ctx ctx);
+int disorder_ctx_set_stream(disorder_ctx ctx, void* cuda_stream); /* NULL: own stream */
+void* disorder_ctx_get_stream(disorder_ctx ctx);
+int disorder_synchronize(disorder_ctx ctx);
+int disorder_malloc(disorder_ctx ctx, size_t bytes, void** dptr);
+int disorder_free(disorder_ctx ctx, void* dptr);
+int disorder_memcpy_h2d(disorder_ctx ctx, void* dst, const void* src, size_t bytes);
+int disorder_memcpy_d2h(disorder_ctx ctx, void* dst, const void* src, size_t bytes);
+/* number of kernels this context has launched since creation */
+int64_t disorder_kernel_launches(disorder_ctx ctx);
+/* CUDA-event timing on the context's stream (no reference counterpart):
+ * disorder_event_record(ctx, slot) records event `slot` (0..15);
+ * disorder_event_elapsed(ctx, a, b, &ms) synchronises on b and returns the
+ * device time between the two events in milliseconds. */
+int disorder_event_record(disorder_ctx ctx, int32_t slot);
+int disorder_event_elapsed(disorder_ctx ctx, int32_t a, int32_t b, float* ms);
+
+/* ---- plan: the geometry and sampling fields of the E structure ----
+ * Replaces generateTransformGrids (Methods/generateTransformGrids.m:23-67:
+ * E.kG, E.rkG) and the sample bookkeeping of buildHarmonicSampling
+ * (Methods/buildHarmonicSampling.m:25-50: E.Fs as DFT-row indices, E.nEc). */
+typedef struct {
+  int32_t N[3];        /* grid size at this level */
+  const float* rG[3];  /* host: rGrid{m}, N[m] values (full-res voxel units) */
+  const float* kG[3];  /* host: kGrid{m}, ifftshifted (sh=1), N[m] values */
+  float cent[3];       /* host: flip centre per dim (cGrid, default N/2+1) */
+} disorder_grid_desc;
+
+typedef struct {
+  int32_t n_seg;              /* E.NSe: segments (motion states + outer) */
+  int32_t n_mot;              /* E.NMs: leading segments with a transform */
+  const int64_t* seg_offsets; /* host: E.nEc, n_seg+1 sample offsets */
+  const int32_t* ky;          /* host: 0-based DFT row of dim 1 per sample */
+  const int32_t* kz;          /* host: 0-based DFT row of dim 2 per sample */
+} disorder_sampling_desc;
+
+int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* grid,
+                         const disorder_sampling_desc* smp, disorder_plan* out);
+int disorder_plan_destroy(disorder_plan plan);
+
+/* ---- sinc rigid transform ----
+ * [x,xB]=sincRigidTransform(x,et,di,F,FH,sumR,useFull) with et from
+ * precomputeFactorsSincRigidTransform(kG,rkG,T,di,0,1,1)
+ * (Methods/sincRigidTransform.m:1-116; Methods/precomputeFactorsSincRigidTransform.m:24-249).
+ * x: device, x_states (1 or n_states) volumes. T: host n_states x 6.
+ * di=1 forward: out holds n_states volumes. di=0 inverse: out holds the sum
+ * over states when sumR!=0, else n_states volumes. useFull: 1 full, 0
+ * translations only, -1 rotations only. */
+int disorder_sinc_rigid_transform(disorder_ctx ctx, disorder_plan plan, const void* x,
+                                  int32_t x_states, const float* T, int32_t n_states,
+                                  int32_t di, int32_t sumR, int32_t useFull, void* out);
+
+/* G=sincRigidTransformGradient(xB,et,etg,F,FH)
+ * (Methods/sincRigidTransformGradient.m:1-150) for the forward transform of
+ * one volume x (device) by n_states transforms T (host). G: device, 6 x
+ * n_states volumes, G[(g*n_states + s)*V]: derivatives with respect to
+ * t1,t2,t3,r1,r2,r3. xT (device, optional): the transformed volumes. */
+int disorder_sinc_rigid_transform_gradient(disorder_ctx ctx, disorder_plan plan,
+                                           const void* x, const float* T, int32_t n_states,
+                                           void* G, void* xT);
+
+/* ---- encoding operators (Reconstruction/encode.m, decode.m, encodedecode.m) ----
+ * Sf: device N1xN2xN3xC. T: host n_mot x 6 or NULL (no motion: the
+ * reference's any(E.Tr(:)~=0) false branch). We: device per-sample weights
+ * (EH.We) or NULL. Mb: device length-N3 readout weights (EH.Mb) or NULL. */
+int disorder_encode(disorder_ctx ctx, disorder_plan plan, const void* x, const void* Sf,
+                    int32_t n_coils, const float* T, void* y);
+int disorder_decode(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
+                    int32_t n_coils, const float* T, const float* We, const float* Mb, void* x);
+int disorder_encodedecode(disorder_ctx ctx, disorder_plan plan, const void* x, const void* Sf,
+                          int32_t n_coils, const float* T, const float* We, void* out);
+
+/* [En]=computeEnergy(y,x,E,R,EH) (Reconstruction/computeEnergy.m:34-80, no=2):
+ * En[0] = sum |sqrt(Mb) sqrt(Mbe) (E x - y)|^2, En[1] = |sum Ti.*|x|^2|.
+ * Mb, Mbe: device length-N3 or NULL. R_Ti: device real V or NULL. En: host. */
+int disorder_compute_energy(disorder_ctx ctx, disorder_plan plan, const void* y, const void* x,
+                            const void* Sf, int32_t n_coils, const float* T, const float* Mb,
+                            const float* Mbe, const float* R_Ti, double* En);
+
+/* ---- solvers ----
+ * [x,En,~,~,nn]=CGsolver(y,E,EH,A,C,R,x,nIt,tolType,tol) with E.Je=1
+ * (Reconstruction/CGsolver.m:1-119). tolType: 1 'RelativeResidual2Error',
+ * 6 'Energy', 7 'None' (Reconstruction/stopCondition.m:10-21).
+ * P_Se (A.Se), C_Ma (C.Ma), R_Ti (R.Ti.la): device real V arrays or NULL.
+ * x_inout: device; used as the initial guess when x_init!=0, else x=0.
+ * En: host, 2 x ceil(nIt/2) doubles (column-major), filled for tolType 6;
+ * n_en, nn: host outputs (energy columns written, iterations run). */
+int disorder_cg_solve(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
+                      int32_t n_coils, const float* T, const float* We, const float* Mb,
+                      const float* Mbe, const float* P_Se, const float* C_Ma, const float* R_Ti,
+                      void* x_inout, int32_t x_init, int32_t nIt, int32_t tolType, double tol,
+                      double* En, int32_t* n_en, int32_t* nn);
+
+/* E=LMsolver(y,E,x,C) (Reconstruction/LMsolver.m:1-226), E.Fs branch, one
+ * Levenberg-Marquardt iteration over the motion states.
+ * y: device samples (all segments, full readout). Sf: device.
+ * x: device volume. T (E.Tr), w (E.w), cT (E.cT): host, updated in place.
+ * winit, tL[2]: E.winit, E.tL. n3_lo/n3_hi: E.nF as the readout range
+ * [n3_lo, n3_hi) (n3_hi<=0: whole readout). En, EnPrev: host n_mot doubles
+ * (energy after/before, per state; E.En = min of the two). */
+int disorder_lm_step(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
+                     int32_t n_coils, const void* x, float* T, float* w, uint8_t* cT,
+                     float winit, const float* tL, int32_t n3_lo, int32_t n3_hi, double* En,
+                     double* EnPrev);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DISORDER_H */

@@ -1,0 +1,220 @@
+"""CGsolver and LMsolver (oracle).
+
+TEST INFRASTRUCTURE ONLY. Restates Reconstruction/CGsolver.m:26-109,
+Reconstruction/stopCondition.m:10-21, Reconstruction/precondition.m:19-23
+(A.Se), Reconstruction/constrain.m:12 (C.Ma), Reconstruction/regularize.m:24
+(Tikhonov R.Ti) and Reconstruction/LMsolver.m:15-226 (the E.Fs branch, motion
+states along dim 5, one block of states).
+"""
+
+import itertools
+
+import numpy as np
+
+from . import encoding as enc
+from .transform import (precomputeFactorsSincRigidTransform, restrictTransform,
+                        sincRigidTransform, sincRigidTransformGradient)
+
+EPS = np.finfo(np.float64).eps
+
+
+def stopCondition(tolType):
+    """Reconstruction/stopCondition.m:10-21 (CG solver)."""
+    table = {"NormwiseBackward2Error": 0, "RelativeResidual2Error": 1, "DataUpdate2Error": 2,
+             "RelativeResidualIError": 3, "DataUpdateIError": 4, "Convergent2Variables": 5,
+             "Energy": 6, "None": 7}
+    t = table.get(tolType, -1)
+    if t in (-1, 5):
+        raise ValueError("The %s stopping criterion is not implemented for CG solver" % tolType)
+    return t
+
+
+def precondition(x, A):
+    """Reconstruction/precondition.m:19-23 (A.Se only)."""
+    if A is None or not A.has("Se"):
+        return x
+    return x * A.Se
+
+
+def constrain(x, C):
+    """Reconstruction/constrain.m:12 (C.Ma only)."""
+    if C is None or not C.has("Ma"):
+        return x
+    return x * C.Ma
+
+
+def regularize(x, R):
+    """Reconstruction/regularize.m:24 (Tikhonov R.Ti.la only)."""
+    if R is None or not R.has("Ti"):
+        return np.zeros_like(x)
+    return R.Ti * x
+
+
+def CGsolver(y, E, EH, A=None, C=None, R=None, x=None, nIt=300, tolType="Energy", tol=1e-5,
+             method="fft", dtype=np.float64):
+    """Reconstruction/CGsolver.m:26-109 with E.Je=1 (encodedecode). Returns
+    (x, En, nn) with En the 2 x k energies sampled every NitTest=2 iterations
+    (empty unless tolType is 'Energy')."""
+    NitTest = 2
+    tolTyp = stopCondition(tolType)
+    b = constrain(enc.decode(y, EH, E, method, dtype), C)  # :46
+    if x is None:  # :53
+        x = np.zeros_like(b)
+        EHE = np.zeros_like(b)
+    else:  # :55
+        x = np.asarray(x, dtype=b.dtype)
+        EHE = constrain(enc.encodedecode(x, E, EH, method, dtype) + regularize(x, R), C)
+    bnorm2 = None
+    if tolTyp not in (6, 7):  # :58-62
+        zb = precondition(b, A)
+        zb = np.conj(zb) * b
+        bnorm2 = np.sum(np.abs(zb))
+    r = b - EHE  # :64
+    z = precondition(r, A)
+    p = z
+    zr = np.conj(z) * r
+    rsold = np.sum(zr)
+    En = np.zeros((2, 0))
+    if abs(rsold) < 1e-6:  # :70-75
+        return x, En, 0
+    err = np.inf
+    if tolTyp == 6:
+        En = np.full((2, nIt), np.inf)
+    n = 0
+    for n in range(1, nIt + 1):  # :79-104
+        EHE = constrain(enc.encodedecode(p, E, EH, method, dtype) + regularize(p, R), C)
+        g = rsold / np.sum(np.conj(p) * EHE)
+        x = x + g * p
+        if n % NitTest == 1 and tolTyp == 6:
+            En[:, n - 1] = enc.computeEnergy(y, x, E, R, EH, method, dtype=dtype)
+        r = r - g * EHE
+        z = precondition(r, A)
+        zr = np.conj(z) * r
+        rs = np.sum(zr)
+        d = rs / (rsold + EPS)
+        p = z + d * p
+        rsold = rs
+        if tolTyp == 1:
+            err = np.sqrt(np.sum(np.abs(zr)) / bnorm2)
+        elif tolTyp == 6 and n % NitTest == 1 and n > 1:
+            err = np.sum(En[:, n - 1 - NitTest] - En[:, n - 1]) / np.sum(En[:, n - 1 - NitTest])
+        if err < tol or abs(rs) < 1e-6:
+            break
+    nn = n
+    if tolTyp == 6:  # :108-109
+        En = En[:, :n]
+    En = En[:, ::NitTest]
+    return x, En, nn
+
+
+# Hessian index pairs ha (LMsolver.m:26): 6 diagonal entries then nchoosek(1:6,2)
+HA = [(i, i) for i in range(6)] + list(itertools.combinations(range(6), 2))
+
+
+def _state_samples(E, vA):
+    return np.concatenate([np.arange(int(E.nEc[s]), int(E.nEc[s + 1])) for s in vA]) if len(vA) else np.zeros(0, int)
+
+
+def _encode_sub(xT, E, vA, method):
+    Es = E.copy(Tr=None, vA=list(vA))
+    return enc.encode(xT, Es, method)
+
+
+def LMsolver(y, E, x, C=None, method="fft", dtype=np.float64, deb=0):
+    """Reconstruction/LMsolver.m:15-226 (E.Fs branch). Returns an updated copy
+    of E with Tr, cT, w and En set as the reference sets them (:217-225).
+
+    Fields used: E.Tr (S x 6), E.cT (S,), E.w (S,), E.winit, E.tL (2,),
+    E.nF (readout indices, optional), E.Sf, E.ky/E.kz/E.nEc, E.mSt, E.grids.
+    """
+    E = E.copy()
+    T = np.asarray(E.Tr, dtype=np.float32).copy()
+    S = T.shape[0]
+    ndG, ndH = 6, len(HA)
+    flagw = np.zeros(S, bool)
+    multA, multB = 1.2, 2.0
+    NElY = y.size  # numel(y) before the readout crop (:32)
+    if E.has("nF"):  # :33
+        nF = np.asarray(E.nF)
+        E = E.copy(Sf=E.Sf[:, :, nF])
+        y = y[:, nF]
+    else:
+        nF = None
+    cTFull = np.asarray(E.cT, bool).copy()
+    w = np.asarray(E.w, np.float64).copy()
+    dH = np.zeros((S, ndH))
+    dG = np.zeros((S, ndG))
+    dGEff = np.zeros((S, ndG))
+    EnPrev = np.zeros(S)
+    ind2EstOr = np.flatnonzero(~cTFull)  # :49
+    vA = list(ind2EstOr)
+
+    def crop(v):
+        return v[:, :, nF] if nF is not None else v
+
+    if vA:
+        indY = _state_samples(E, vA)
+        Tf, Tg = precomputeFactorsSincRigidTransform(E.grids, T[vA], 1, 1, dtype)  # :60
+        xT, xB = sincRigidTransform(x, Tf, 1, keep_intermediates=True)  # :66
+        r = _encode_sub(crop(xT), E, vA, method) - y[indY]  # :72
+        ry = np.sum(np.abs(r) ** 2, axis=(1, 2)) / NElY  # :82
+        mst = np.asarray(E.mSt)[indY]
+        EnPrev[vA] = np.bincount(mst, ry, minlength=S)[vA]  # :83,93
+        G = sincRigidTransformGradient(xB, Tf, Tg)  # :96
+        Genc = [_encode_sub(crop(g), E, vA, method) for g in G]  # :97-99
+        for gi in range(ndG):  # :106
+            v = np.sum(np.real(Genc[gi] * np.conj(r)), axis=(1, 2))
+            dG[vA, gi] = np.bincount(mst, v, minlength=S)[vA]
+        for h, (a_, b_) in enumerate(HA):  # :115
+            v = np.sum(np.real(Genc[a_] * np.conj(Genc[b_])), axis=(1, 2))
+            dH[vA, h] = np.bincount(mst, v, minlength=S)[vA]
+
+    En = EnPrev.copy()
+    MH = np.eye(ndG)
+    fina = False
+    Tupr = np.zeros_like(T)
+    Tup = T
+    while not fina:  # :129-215
+        for a in np.flatnonzero(~cTFull & (w < 1e10)):
+            for h, (p_, q_) in enumerate(HA):
+                if p_ == q_:
+                    MH[p_, q_] = (1 + w[a]) * dH[a, h]
+                else:
+                    MH[p_, q_] = dH[a, h]
+                    MH[q_, p_] = dH[a, h]
+            GJ = np.linalg.solve(MH, dG[a])
+            dGEff[a] = -(E.winit / w[a]) * GJ
+        Tupr = dGEff.astype(np.float32)
+        Tup = restrictTransform(T + Tupr)  # :143
+        ecT = cTFull | flagw  # :146
+        vE = list(np.flatnonzero(~ecT))
+        if vE:
+            indY = _state_samples(E, vE)
+            Tf, _ = precomputeFactorsSincRigidTransform(E.grids, Tup[vE], 1, 0, dtype)
+            xT = sincRigidTransform(x, Tf, 1)
+            r = _encode_sub(crop(xT), E, vE, method) - y[indY]
+            ry = np.sum(np.abs(r) ** 2, axis=(1, 2)) / NElY
+            mst = np.asarray(E.mSt)[indY]
+            En[vE] = np.bincount(mst, ry, minlength=S)[vE]
+        En[w > 1e10] = EnPrev[w > 1e10]  # :195
+        flagw[En <= EnPrev] = True  # :196
+        if deb >= 2:
+            print("Energy before: %0.6g / Energy after: %0.6g" % (EnPrev.sum(), En.sum()))
+        if np.any(~flagw):  # :199-200
+            sel = (En > EnPrev) & ~cTFull
+            w[sel] = w[sel] * multB
+        else:  # :201-213
+            w[~cTFull] = w[~cTFull] / multA
+            w[w < 1e-8] = multA * w[w < 1e-8]
+            T = Tup
+            fina = True
+            traDiff = np.abs(Tupr[:, 0:3])
+            rotDiff = np.abs(Tupr[:, 3:6] * 180 / np.pi)
+            cTFull[(traDiff.max(axis=1) < E.tL[0]) & (rotDiff.max(axis=1) < E.tL[1])] = True
+    Enmin = np.minimum(EnPrev, En)  # :224-225
+    if E.has("En"):
+        Eo = np.asarray(E.En, float).copy()
+        Eo[ind2EstOr] = Enmin[ind2EstOr]
+    else:
+        Eo = Enmin
+    return E.copy(Tr=T.astype(np.float32), cT=cTFull, w=w, En=Eo, EnPrev=EnPrev)
