@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark: seconds per 3-D motion-corrected (aligned) reconstruction.
+
+Workload (plain method on GPU, FP32 complex): a seeded synthetic
+256x256x176 scan (40 random ellipsoids, smooth random phase), 32 Gaussian-bump
+coils compressed to 16, 64 random-checkered shots, per-shot rotations
+U(-5,5) deg and translations U(-5,5) voxels (1 mm), complex noise at 25 dB
+SNR. One step is one full aligned reconstruction: coil compression, a 3-level
+resolution pyramid (64x64x44, 128x128x88, 256x256x176) with up to 20 outer
+iterations of CG + Levenberg-Marquardt motion estimation at the two coarse
+levels and a final CG (energy tolerance 1e-3) at full resolution.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+For N > 1 (one process per GPU under torchrun) each GPU reconstructs its own
+scan (replicas; the path's multi-GPU shot sharding is not built): value is
+seconds per reconstruction of the whole job (time / N).
+"""
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s per 3D aligned recon to plain-method NRMSE: learned+mixed vs plain, 1 B200"
+CFG = dict(N=(256, 256, 176), coils=32, coils_kept=16, shots=64, rot_deg=5.0, trans_vox=5.0, snr_db=25.0,
+           ellipsoids=40, seed=2000)
+SMALL = dict(N=(64, 64, 48), coils=8, coils_kept=6, shots=16, rot_deg=5.0, trans_vox=3.0, snr_db=25.0,
+             ellipsoids=12, seed=2001)
+NOMINAL_COUNTS = {"outer": [20, 20], "cg_final": 30}  # nominal schedule for the CPU reference estimate
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, gpu_index=0):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+        self.gpu = gpu_index
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- scan synthesis
+def build_scan(ctx, cfg, use_torch=True):
+    """Synthesise the scan on the GPU: x_gt, 32 coils, shot map, motion and
+    noisy samples y = encode(x_gt) + noise (Simulation/synthesizeY.m:82-84)."""
+    import disorder_b200 as db
+    from disorder_b200 import synth
+    N = tuple(cfg["N"])
+    rng = np.random.default_rng(cfg["seed"])
+    sc = synth.Scan()
+    sc.N = N
+    if use_torch:
+        import torch
+        from disorder_b200 import synth_gpu
+        dev = "cuda:%d" % ctx.device
+        xt = synth_gpu.phantom_torch(N, cfg["ellipsoids"], rng, dev).to(torch.complex64)
+        St = synth_gpu.coils_torch(N, cfg["coils"], rng, dev=dev)
+        sigma = _sigma_torch(cfg["snr_db"], xt, St)
+        x_gt = ctx.empty(N)
+        S = ctx.empty(N + (cfg["coils"],))
+        xf = xt.permute(2, 1, 0).contiguous()
+        Sf = St.permute(3, 2, 1, 0).contiguous()
+        torch.cuda.synchronize()
+        ctx.check(ctx.lib.disorder_memcpy_d2d(ctx.h, x_gt.ptr, xf.data_ptr(), x_gt.nbytes))
+        ctx.check(ctx.lib.disorder_memcpy_d2d(ctx.h, S.ptr, Sf.data_ptr(), S.nbytes))
+        ctx.synchronize()
+        del xf, Sf, St
+        sc.x_gt_host = xt.cpu().numpy()
+        del xt
+    else:
+        xh = synth.phantom(N, cfg["ellipsoids"], rng)
+        xh = (xh / np.linalg.norm(xh.ravel())).astype(np.complex64)
+        Sh = synth.coil_maps(N, cfg["coils"], rng)
+        sigma = synth.snr_to_sigma(cfg["snr_db"], xh, Sh)
+        x_gt = ctx.upload(xh)
+        S = ctx.upload(Sh)
+        sc.x_gt_host = xh
+    sc.H = synth.random_checkered(N[:2], cfg["shots"], rng)
+    sc.ky, sc.kz, sc.nEc, sc.mSt, sc.iSt = synth.sample_lists(sc.H, cfg["shots"])
+    sc.T_gt = synth.motion(cfg["shots"], cfg["rot_deg"], cfg["trans_vox"], rng)
+    sc.sigma = sigma
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    E = db.Struct(Tr=sc.T_gt, NMs=cfg["shots"], NSe=cfg["shots"] + 1, Sf=S, grids=db.generateTransformGrids(N, N, cent),
+                  ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt)
+    y = db.encode(x_gt, E, ctx=ctx)
+    if use_torch:
+        import torch
+        yt = torch.empty(y.nbytes // 8, dtype=torch.complex64, device="cuda:%d" % ctx.device)
+        ctx.check(ctx.lib.disorder_memcpy_d2d(ctx.h, yt.data_ptr(), y.ptr, y.nbytes))
+        ctx.synchronize()
+        g = torch.Generator(device=yt.device)
+        g.manual_seed(cfg["seed"] + 7919)
+        yt += sigma * torch.complex(torch.randn(yt.shape, generator=g, device=yt.device),
+                                    torch.randn(yt.shape, generator=g, device=yt.device))
+        torch.cuda.synchronize()
+        ctx.check(ctx.lib.disorder_memcpy_d2d(ctx.h, y.ptr, yt.data_ptr(), y.nbytes))
+        ctx.synchronize()
+        del yt
+    else:
+        yh = synth.add_noise(y.numpy(), sigma, cfg["seed"] + 7919)
+        y = ctx.upload(yh)
+    sc.x_gt, sc.S, sc.y = x_gt, S, y
+    return sc
+
+
+def _sigma_torch(snr_db, x, S):
+    """Simulation/SNRToLevels.m:23-33 on torch tensors, for the unitary
+    encoding (see disorder_b200.synth.snr_to_sigma)."""
+    import torch
+    meanS = torch.mean(torch.abs(x) ** 2).item()
+    meanN = meanS / (10 ** (snr_db / 10))
+    P = torch.mean(1.0 / (torch.sum(torch.abs(S) ** 2, dim=3) + 1e-3)).item()
+    return float(math.sqrt(meanN / (2 * P)))
+
+
+def nrmse(ctx, x, x_gt_host):
+    xh = x.numpy()
+    return float(np.linalg.norm((xh - x_gt_host).ravel()) / np.linalg.norm(x_gt_host.ravel()))
+
+
+# ---------------------------------------------------------------- CPU baseline (oracle, FP64)
+def cpu_estimate(N, n_states, C, counts, budget_note=True):
+    """Time the FP64 NumPy restatement (oracle) on bounded samples of the
+    workload and extrapolate to one reconstruction with the given schedule:
+    counts = {"outer": [n_outer_L1, n_outer_L2], "cg_final": n}. Samples: the
+    normal operator (encodedecode) for 8 of the 64 states at 64x64x44, the LM
+    step for 8 states at 64x64x44, and the normal operator for 1 state at the
+    full size; other levels and state counts are scaled by voxel count and
+    state count. Returns (seconds per reconstruction, threads, description)."""
+    from disorder_b200 import synth
+    from oracle import encoding as oenc
+    from oracle import grids as og
+    from oracle import solvers as osol
+    threads = os.cpu_count() or 1
+    og.WORKERS = threads
+
+    def problem(Nl, S_sub, seed):
+        rng = np.random.default_rng(seed)
+        x = (rng.standard_normal(Nl) + 1j * rng.standard_normal(Nl))
+        Sf = (rng.standard_normal(Nl + (C,)) + 1j * rng.standard_normal(Nl + (C,)))
+        H = synth.random_checkered(Nl[:2], n_states, rng)
+        ky, kz, nEc, mSt, _ = synth.sample_lists(H, n_states)
+        T = synth.motion(n_states, 5, 5, rng)
+        cent = [math.ceil((n + 1) / 2.0) for n in Nl]
+        g = og.generateTransformGrids(N, Nl, cent, sh=1)
+        E = oenc.Struct(Tr=T, NMs=n_states, NSe=n_states + 1, Sf=Sf, ky=ky, kz=kz, nEc=nEc, mSt=mSt, grids=g,
+                        vA=list(range(S_sub)))
+        return x, E
+
+    L1 = tuple(int(math.ceil(n / 4)) for n in N)
+    L2 = tuple(int(math.ceil(n / 2)) for n in N)
+    sub = 8
+    x1, E1 = problem(L1, sub, 1)
+    t0 = time.perf_counter()
+    oenc.encodedecode(x1, E1, None)
+    t_ed1 = (time.perf_counter() - t0) * n_states / sub
+    # LM step for `sub` states
+    y1 = oenc.encode(x1, E1.copy(vA=None))
+    Elm = E1.copy(vA=None, Tr=E1.Tr, cT=np.arange(n_states) >= sub, w=np.full(n_states, 1e-3), winit=1e-3,
+                  tL=[0.05, 0.02], nF=np.arange(0, int(2 * L1[2] / 3)))
+    t0 = time.perf_counter()
+    osol.LMsolver(y1, Elm, x1)
+    t_lm1 = (time.perf_counter() - t0) * n_states / sub
+    x3, E3 = problem(tuple(N), 1, 3)
+    t0 = time.perf_counter()
+    oenc.encodedecode(x3, E3, None)
+    t_ed3 = (time.perf_counter() - t0) * n_states
+    v1, v2, v3 = np.prod(L1), np.prod(L2), np.prod(N)
+    t_ed2, t_lm2 = t_ed1 * v2 / v1, t_lm1 * v2 / v1
+    # per outer iteration at a motion level: CG with 1 iteration (decode + 2 normal operators ~ 2.5 ED) + LM
+    per_outer = [2.5 * t_ed1 + t_lm1, 2.5 * t_ed2 + t_lm2]
+    est = counts["outer"][0] * per_outer[0] + counts["outer"][1] * per_outer[1] + (counts["cg_final"] + 2) * t_ed3
+    desc = ("FP64 NumPy restatement (oracle), %d threads; timed: encodedecode 8/%d states at %s, LM step 8/%d states "
+            "at %s, encodedecode 1/%d states at %s; extrapolated by state count and voxel count to the schedule "
+            "%s" % (threads, n_states, "x".join(map(str, L1)), n_states, "x".join(map(str, L1)), n_states,
+                    "x".join(map(str, N)), json.dumps(counts)))
+    return est, threads, desc
+
+
+# ---------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--small", action="store_true", help="small scan (functional check)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    cfg = SMALL if args.small else CFG
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": "aligned recon %s, %d coils -> %d, %d shots, 3-level pyramid, plain FP32"
+                          % ("x".join(map(str, cfg["N"])), cfg["coils"], cfg["coils_kept"], cfg["shots"]),
+              "N": list(cfg["N"]), "coils": cfg["coils"], "coils_kept": cfg["coils_kept"], "shots": cfg["shots"],
+              "l2_flush": "inputs larger than L2 (coil maps and samples are GB-sized)", "parallelism": "replicas"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        vals = []
+        for it in range(args.warmup + args.steps):
+            est, thr, desc = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], NOMINAL_COUNTS)
+            if it >= args.warmup:
+                vals.append(est)
+        v = float(np.mean(vals))
+        print(json.dumps({"metric": METRIC, "value": v, "unit": "s", "impl": "reference", "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+                          "higher_is_better": False, "dtype": "f64", "data": "synthetic", "config": config,
+                          "cpu_baseline": {"value": v, "unit": "s", "cores": thr, "kind": "port", "sample": desc},
+                          "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                          "vs_baseline": None}))
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    import disorder_b200 as db
+    from disorder_b200 import recon
+    ctx = db.Context(local)
+    cfg_r = dict(cfg)
+    cfg_r["seed"] = cfg["seed"] + 97 * rank
+    sc = build_scan(ctx, cfg_r, use_torch=True)
+
+    def one(S, y):
+        return recon.aligned_reconstruction(ctx, S, y, sc.H, cfg["shots"], cfg["N"], perc=cfg["coils_kept"])
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        x, T, log = one(sc.S, sc.y)
+    ctx.synchronize()
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    l0 = ctx.launches
+    ctx.event(0)
+    logs = []
+    for _ in range(args.steps):
+        x, T, log = one(sc.S, sc.y)
+        logs.append(log)
+    ctx.event(1)
+    ms_total = ctx.elapsed_ms(0, 1)
+    launches = ctx.launches - l0
+    clocks = clk.stop()
+    barrier()
+    ms = ms_total / args.steps
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda:%d" % local)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    err = nrmse(ctx, x, sc.x_gt_host)
+    motion_err = float(np.max(np.abs(T - sc.T_gt)[:, :3])), float(np.degrees(np.max(np.abs(T - sc.T_gt)[:, 3:])))
+    counts = {"outer": [sum(1 for e in logs[-1].events if e["step"] == "lm" and e["level"] == lv) for lv in (0, 1)],
+              "cg_final": sum(e["iters"] for e in logs[-1].events if e["step"] == "cg" and e["level"] == 2)}
+
+    # end to end through the public API with host buffers (upload, recon, download)
+    Sh = sc.S.numpy()
+    yh = sc.y.numpy()
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    ctx.event(2)
+    Sd = ctx.upload(Sh)
+    yd = ctx.upload(yh)
+    xe, _, _ = one(Sd, yd)
+    xh = xe.numpy()
+    ctx.event(3)
+    e2e_ms = ctx.elapsed_ms(2, 3)
+    del Sd, yd, xh
+
+    # roofline of the dominant kernel family: the line passes of the sinc rigid
+    # transform at full size (11 passes per forward transform, each reading
+    # and writing the 64 state volumes)
+    N = cfg["N"]
+    V = int(np.prod(N))
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    et, _ = db.precomputeFactorsSincRigidTransform(db.generateTransformGrids(N, N, cent), sc.T_gt, 1)
+    xg = sc.x_gt
+    outt, _ = db.sincRigidTransform(xg, et, 1, ctx=ctx)
+    ctx.synchronize()
+    reps = 3
+    ctx.event(4)
+    for _ in range(reps):
+        outt, _ = db.sincRigidTransform(xg, et, 1, ctx=ctx)
+    ctx.event(5)
+    t_fwd = ctx.elapsed_ms(4, 5) / reps
+    del outt
+    n_pass = 11
+    bytes_per_launch = 16.0 * V * cfg["shots"]
+    achieved = bytes_per_launch / (t_fwd / n_pass * 1e-3) / 1e9
+    peak, pkind = peaks()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "fp::line_kernel (sinc-transform line pass)",
+            "peak_kind": pkind, "bytes_per_launch": bytes_per_launch}
+
+    out = {"metric": METRIC, "value": ms * 1e-3 / world, "unit": "s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic", "config": config,
+           "nrmse": err, "motion_max_err": {"trans_vox": motion_err[0], "rot_deg": motion_err[1]},
+           "schedule": counts, "gpu_launches": int(launches / args.steps), "clocks": clocks,
+           "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": int(Sh.nbytes + yh.nbytes),
+                   "d2h_bytes_per_step": int(V * 8)},
+           "roofline": roof}
+    if rank == 0 and not args.no_cpu:
+        est, thr, desc = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], counts)
+        out["cpu_baseline"] = {"value": est, "unit": "s", "cores": thr, "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -10,5 +10,6 @@ the library and fails loudly if it is missing.
 
 from .api import (CGsolver, Context, DeviceArray, Grids, LMsolver, Plan, Struct, computeEnergy, decode,  # noqa: F401
                   default_context, encode, encodedecode, generateTransformGrids,
-                  precomputeFactorsSincRigidTransform, sincRigidTransform, sincRigidTransformGradient)
+                  precomputeFactorsSincRigidTransform, sincRigidTransform, sincRigidTransformGradient,
+                  compressCoils, gather_samples, precondition_weights, resampling)
 from ._lib import DisorderError  # noqa: F401

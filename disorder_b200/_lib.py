@@ -50,6 +50,8 @@ SIGNATURES = [
     ("disorder_free", C.c_int, [VP, VP]),
     ("disorder_memcpy_h2d", C.c_int, [VP, VP, VP, C.c_size_t]),
     ("disorder_memcpy_d2h", C.c_int, [VP, VP, VP, C.c_size_t]),
+    ("disorder_memcpy_d2d", C.c_int, [VP, VP, VP, C.c_size_t]),
+    ("disorder_memset", C.c_int, [VP, VP, C.c_int, C.c_size_t]),
     ("disorder_kernel_launches", C.c_int64, [VP]),
     ("disorder_event_record", C.c_int, [VP, I32]),
     ("disorder_event_elapsed", C.c_int, [VP, I32, I32, FP]),
@@ -65,6 +67,11 @@ SIGNATURES = [
                                     DP, C.POINTER(I32), C.POINTER(I32)]),
     ("disorder_lm_step", C.c_int, [VP, VP, VP, VP, I32, VP, FP, FP, C.POINTER(C.c_uint8), C.c_float, FP, I32, I32,
                                    DP, DP]),
+    ("disorder_resample", C.c_int, [VP, VP, C.POINTER(I32), I32, C.POINTER(I32), VP]),
+    ("disorder_gather_samples", C.c_int, [VP, VP, C.c_int64, C.c_int64, VP, C.c_int64, C.c_float, VP]),
+    ("disorder_precondition_weights", C.c_int, [VP, VP, I32, C.c_int64, C.c_float, VP]),
+    ("disorder_compress_coils", C.c_int, [VP, VP, I32, C.c_int64, VP, C.c_int64, C.c_double, I32, VP, VP,
+                                          C.POINTER(I32), DP, DP]),
 ]
 
 _lib = None

@@ -494,3 +494,68 @@ def sincRigidTransformGradient(xB, et, etg=None, ctx=None):
     T = _fptr(et.T)
     ctx.check(ctx.lib.disorder_sinc_rigid_transform_gradient(ctx.h, p.h, xd.ptr, T[1], S, G.ptr, None))
     return _out(G, host)
+
+
+# ---------------------------------------------------------------- data preparation
+def resampling(x, Nres, n_vols=None, ctx=None):
+    """Methods/resampling.m:45-94 for image-space complex data (fo=0): Fourier
+    crop/zero-pad of each volume to Nres. x: (N1,N2,N3) or (N1,N2,N3,K)."""
+    ctx = ctx or default_context()
+    xd, host = _dev(ctx, x, np.complex64)
+    shp = tuple(xd.shape[:3]) + (1,) * (3 - len(xd.shape[:3]))
+    K = int(np.prod(xd.shape[3:])) if len(xd.shape) > 3 else 1
+    Nres = tuple(int(n) for n in Nres)
+    out = ctx.empty(Nres + tuple(xd.shape[3:]))
+    nin = (C.c_int32 * 3)(*shp)
+    nout = (C.c_int32 * 3)(*Nres)
+    ctx.check(ctx.lib.disorder_resample(ctx.h, xd.ptr, nin, K, nout, out.ptr))
+    return _out(out, host)
+
+
+def compressCoils(S, perc, y=None, C_max=0, ctx=None):
+    """Methods/compressCoils.m:76-118: returns (S, y, C, D, U)."""
+    ctx = ctx or default_context()
+    Sd, host = _dev(ctx, S, np.complex64)
+    Cin = Sd.shape[-1]
+    V = int(np.prod(Sd.shape[:-1]))
+    yd, _ = _dev(ctx, y, np.complex64)
+    So = ctx.empty(Sd.shape)
+    yo = ctx.empty(yd.shape) if yd is not None else None
+    Cout = C.c_int32()
+    D = (C.c_double * Cin)()
+    U = (C.c_double * (2 * Cin * Cin))()
+    ny = int(np.prod(yd.shape[:-1])) if yd is not None else 0
+    ctx.check(ctx.lib.disorder_compress_coils(ctx.h, Sd.ptr, Cin, V, yd.ptr if yd else None, ny, float(perc),
+                                              int(C_max), So.ptr, yo.ptr if yo else None, C.byref(Cout), D, U))
+    c = Cout.value
+    Sv = So.view(0, tuple(Sd.shape[:-1]) + (c,))
+    yv = yo.view(0, tuple(yd.shape[:-1]) + (c,)) if yo is not None else None
+    Um = np.array(U[:]).reshape(-1, 2)
+    Um = (Um[:, 0] + 1j * Um[:, 1]).reshape(Cin, Cin, order="F")
+    if host:
+        Sv = Sv.numpy()
+        yv = yv.numpy() if yv is not None else None
+    return Sv, yv, c, np.array(D[:]), Um
+
+
+def precondition_weights(Sf, reg=1e-9, ctx=None):
+    """A.Se = 1 ./ (sum_c |S_c|^2 + reg) (Reconstruction/solveXT.m:231-233)."""
+    ctx = ctx or default_context()
+    Sd, host = _dev(ctx, Sf, np.complex64)
+    V = int(np.prod(Sd.shape[:3]))
+    Cn = Sd.shape[3] if len(Sd.shape) > 3 else 1
+    out = ctx.empty(Sd.shape[:3], np.float32)
+    ctx.check(ctx.lib.disorder_precondition_weights(ctx.h, Sd.ptr, Cn, V, float(reg), out.ptr))
+    return _out(out, host)
+
+
+def gather_samples(y, idx, scale, ctx=None):
+    """Rows idx of a (Ns, N3, C) sample array times scale (a pyramid-level crop)."""
+    ctx = ctx or default_context()
+    yd, host = _dev(ctx, y, np.complex64)
+    idx_d = ctx.upload(np.asarray(idx, np.int32))
+    rows = int(np.prod(yd.shape[1:]))
+    out = ctx.empty((len(idx),) + tuple(yd.shape[1:]))
+    ctx.check(ctx.lib.disorder_gather_samples(ctx.h, yd.ptr, yd.shape[0], rows, idx_d.ptr, len(idx), float(scale),
+                                              out.ptr))
+    return _out(out, host)

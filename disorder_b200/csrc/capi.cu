@@ -1,6 +1,7 @@
 // C ABI of libdisorder: contexts, workspaces, plans and the entry points
 // declared in include/disorder.h.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstring>
 #include <numeric>
@@ -172,6 +173,20 @@ int disorder_memcpy_d2h(disorder_ctx ctx, void* dst, const void* src, size_t byt
   return DISORDER_OK;
 }
 
+int disorder_memcpy_d2d(disorder_ctx ctx, void* dst, const void* src, size_t bytes) {
+  CTX_CHECK(ctx);
+  DEV_GUARD(ctx);
+  DIS_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  return DISORDER_OK;
+}
+
+int disorder_memset(disorder_ctx ctx, void* dst, int value, size_t bytes) {
+  CTX_CHECK(ctx);
+  DEV_GUARD(ctx);
+  DIS_CUDA_TRY(cudaMemsetAsync(dst, value, bytes, ctx->stream));
+  return DISORDER_OK;
+}
+
 int64_t disorder_kernel_launches(disorder_ctx ctx) { return ctx ? ctx->launches : -1; }
 
 int disorder_event_record(disorder_ctx ctx, int32_t slot) {
@@ -224,6 +239,15 @@ int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* g, const di
       return fail(dis_set_error(ctx, DISORDER_OOM, "plan: grid allocation"));
     cudaMemcpy(p->d_kG[m], p->kG[m].data(), sizeof(float) * p->N[m], cudaMemcpyHostToDevice);
     cudaMemcpy(p->d_rG[m], p->rG[m].data(), sizeof(float) * p->N[m], cudaMemcpyHostToDevice);
+    // twiddles exp(-2 pi i j / N) in double precision, rounded to single
+    std::vector<float2> tw(p->N[m]);
+    for (int j = 0; j < p->N[m]; ++j) {
+      const double ang = -2.0 * M_PI * (double)j / (double)p->N[m];
+      tw[j] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+    if (cudaMalloc(&p->d_tw[m], sizeof(float2) * p->N[m]) != cudaSuccess)
+      return fail(dis_set_error(ctx, DISORDER_OOM, "plan: twiddle allocation"));
+    cudaMemcpy(p->d_tw[m], tw.data(), sizeof(float2) * p->N[m], cudaMemcpyHostToDevice);
   }
   // sampling
   if (smp->n_seg < 0 || smp->n_mot < 0 || smp->n_mot > smp->n_seg || !smp->seg_offsets)
@@ -276,6 +300,7 @@ int disorder_plan_destroy(disorder_plan p) {
   for (int m = 0; m < 3; ++m) {
     cudaFree(p->d_kG[m]);
     cudaFree(p->d_rG[m]);
+    cudaFree(p->d_tw[m]);
   }
   cudaFree(p->d_ky);
   cudaFree(p->d_kz);

@@ -5,6 +5,7 @@
 // reference (Fs{1}, Fs{2}: rows of build1DFTM(N,1)) are evaluated as a full
 // FFT along dim 1 followed by an FFT along dim 2 and a gather of each
 // segment's samples, which is the same linear map.
+#include "fastpass.h"
 #include "internal.h"
 
 namespace {
@@ -286,6 +287,12 @@ void ensure_attrs() { static AttrInit once; }
 
 int dis_coil_expand_fft1(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* z,
                          float2* A) {
+  if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
+  if (dis_use_fast() && dis_fast_expand(a.N1, a, z, A, plan->d_tw[0], ctx->stream)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   ensure_attrs();
   const int n = a.N1;
   const int L = pick_L(n, 3);
@@ -300,6 +307,13 @@ int dis_coil_expand_fft1(disorder_ctx_s* ctx, const disorder_plan_s* plan, const
 
 int dis_coil_fft2_gather(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* A,
                          float2* y, long long y_ld, int y_n3off, int y_N3, const float2* y_meas, float scale) {
+  if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
+  if (dis_use_fast() && dis_fast_axis1(a.N2, 0, a, const_cast<float2*>(A), y, y_meas, y_ld, y_n3off, y_N3, scale,
+                                       nullptr, nullptr, nullptr, plan, plan->d_tw[1], ctx->stream)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   ensure_attrs();
   const int n = a.N2;
   const int L = pick_L(n, 2);
@@ -315,6 +329,13 @@ int dis_coil_fft2_gather(disorder_ctx_s* ctx, const disorder_plan_s* plan, const
 
 int dis_coil_scatter_ifft2(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* y,
                            long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* A) {
+  if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
+  if (dis_use_fast() && dis_fast_axis1(a.N2, 2, a, A, const_cast<float2*>(y), nullptr, y_ld, y_n3off, y_N3, 1.f,
+                                       nullptr, We, Mb, plan, plan->d_tw[1], ctx->stream)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   ensure_attrs();
   const int n = a.N2;
   const int L = pick_L(n, 2);
@@ -329,6 +350,15 @@ int dis_coil_scatter_ifft2(disorder_ctx_s* ctx, const disorder_plan_s* plan, con
 
 int dis_coil_fft2_weight(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, float2* A,
                          const float* wmap) {
+  if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
+  // the fast kernel applies w and the explicit inverse; the 1/(N1*N2) of the
+  // inverse DFTs is applied by the combine step
+  if (dis_use_fast() && dis_fast_axis1(a.N2, 1, a, A, nullptr, nullptr, 0, 0, 0, 1.f, wmap, nullptr, nullptr, plan,
+                                       plan->d_tw[1], ctx->stream)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   ensure_attrs();
   const int n = a.N2;
   const int L = pick_L(n, 2);
@@ -342,6 +372,12 @@ int dis_coil_fft2_weight(disorder_ctx_s* ctx, const disorder_plan_s* plan, const
 
 int dis_coil_ifft1_combine(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* A,
                            float2* u, float scale) {
+  if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
+  if (dis_use_fast() && dis_fast_combine(a.N1, a, A, u, scale, plan->d_tw[0], ctx->stream)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   ensure_attrs();
   const int n = a.N1;
   const int L = pick_L(n, 3);

@@ -1,0 +1,104 @@
+// Size dispatch of the register-resident line-pass kernels. The kernels are
+// instantiated in fast_[a-e].cu (one translation unit per group of sizes).
+#include "fastpass.cuh"
+#include "fastpass.h"
+
+extern template struct fp::Launch<4, 4>;
+extern template struct fp::Launch<8, 4>;
+extern template struct fp::Launch<4, 11>;
+extern template struct fp::Launch<8, 8>;
+extern template struct fp::Launch<8, 11>;
+extern template struct fp::Launch<8, 12>;
+extern template struct fp::Launch<16, 8>;
+extern template struct fp::Launch<16, 10>;
+extern template struct fp::Launch<16, 11>;
+extern template struct fp::Launch<16, 12>;
+extern template struct fp::Launch<16, 16>;
+
+bool dis_fast_factor(int n, int* F1, int* F2) {
+  switch (n) {
+    case 16: *F1 = 4; *F2 = 4; return true;
+    case 32: *F1 = 8; *F2 = 4; return true;
+    case 44: *F1 = 4; *F2 = 11; return true;
+    case 64: *F1 = 8; *F2 = 8; return true;
+    case 88: *F1 = 8; *F2 = 11; return true;
+    case 96: *F1 = 8; *F2 = 12; return true;
+    case 128: *F1 = 16; *F2 = 8; return true;
+    case 160: *F1 = 16; *F2 = 10; return true;
+    case 176: *F1 = 16; *F2 = 11; return true;
+    case 192: *F1 = 16; *F2 = 12; return true;
+    case 256: *F1 = 16; *F2 = 16; return true;
+    default: return false;
+  }
+}
+
+bool dis_fast_line(const LinePassArgs& a, const float2* tw, cudaStream_t s) {
+  switch (a.N[a.axis]) {
+    case 16: fp::Launch<4, 4>::line(a, tw, s); return true;
+    case 32: fp::Launch<8, 4>::line(a, tw, s); return true;
+    case 44: fp::Launch<4, 11>::line(a, tw, s); return true;
+    case 64: fp::Launch<8, 8>::line(a, tw, s); return true;
+    case 88: fp::Launch<8, 11>::line(a, tw, s); return true;
+    case 96: fp::Launch<8, 12>::line(a, tw, s); return true;
+    case 128: fp::Launch<16, 8>::line(a, tw, s); return true;
+    case 160: fp::Launch<16, 10>::line(a, tw, s); return true;
+    case 176: fp::Launch<16, 11>::line(a, tw, s); return true;
+    case 192: fp::Launch<16, 12>::line(a, tw, s); return true;
+    case 256: fp::Launch<16, 16>::line(a, tw, s); return true;
+    default: return false;
+  }
+}
+
+bool dis_fast_expand(int n, const CoilArgs& a, const float2* z, float2* A, const float2* tw, cudaStream_t s) {
+  switch (n) {
+    case 16: fp::Launch<4, 4>::expand(a, z, A, tw, s); return true;
+    case 32: fp::Launch<8, 4>::expand(a, z, A, tw, s); return true;
+    case 44: fp::Launch<4, 11>::expand(a, z, A, tw, s); return true;
+    case 64: fp::Launch<8, 8>::expand(a, z, A, tw, s); return true;
+    case 88: fp::Launch<8, 11>::expand(a, z, A, tw, s); return true;
+    case 96: fp::Launch<8, 12>::expand(a, z, A, tw, s); return true;
+    case 128: fp::Launch<16, 8>::expand(a, z, A, tw, s); return true;
+    case 160: fp::Launch<16, 10>::expand(a, z, A, tw, s); return true;
+    case 176: fp::Launch<16, 11>::expand(a, z, A, tw, s); return true;
+    case 192: fp::Launch<16, 12>::expand(a, z, A, tw, s); return true;
+    case 256: fp::Launch<16, 16>::expand(a, z, A, tw, s); return true;
+    default: return false;
+  }
+}
+
+bool dis_fast_combine(int n, const CoilArgs& a, const float2* A, float2* u, float scale, const float2* tw,
+                      cudaStream_t s) {
+  switch (n) {
+    case 16: fp::Launch<4, 4>::combine(a, A, u, scale, tw, s); return true;
+    case 32: fp::Launch<8, 4>::combine(a, A, u, scale, tw, s); return true;
+    case 44: fp::Launch<4, 11>::combine(a, A, u, scale, tw, s); return true;
+    case 64: fp::Launch<8, 8>::combine(a, A, u, scale, tw, s); return true;
+    case 88: fp::Launch<8, 11>::combine(a, A, u, scale, tw, s); return true;
+    case 96: fp::Launch<8, 12>::combine(a, A, u, scale, tw, s); return true;
+    case 128: fp::Launch<16, 8>::combine(a, A, u, scale, tw, s); return true;
+    case 160: fp::Launch<16, 10>::combine(a, A, u, scale, tw, s); return true;
+    case 176: fp::Launch<16, 11>::combine(a, A, u, scale, tw, s); return true;
+    case 192: fp::Launch<16, 12>::combine(a, A, u, scale, tw, s); return true;
+    case 256: fp::Launch<16, 16>::combine(a, A, u, scale, tw, s); return true;
+    default: return false;
+  }
+}
+
+bool dis_fast_axis1(int n, int mode, const CoilArgs& a, float2* A, float2* y, const float2* ymeas, long long ld,
+                    int n3off, int N3y, float scale, const float* wmap, const float* We, const float* Mb,
+                    const disorder_plan_s* plan, const float2* tw, cudaStream_t s) {
+  switch (n) {
+    case 16: fp::Launch<4, 4>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 32: fp::Launch<8, 4>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 44: fp::Launch<4, 11>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 64: fp::Launch<8, 8>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 88: fp::Launch<8, 11>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 96: fp::Launch<8, 12>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 128: fp::Launch<16, 8>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 160: fp::Launch<16, 10>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 176: fp::Launch<16, 11>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 192: fp::Launch<16, 12>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    case 256: fp::Launch<16, 16>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
+    default: return false;
+  }
+}

@@ -67,7 +67,11 @@ struct disorder_plan_s {
   int* d_perm = nullptr;
   int* d_seg_of = nullptr;  // segment of each sample
   long long* d_seg_off = nullptr;
+  float2* d_tw[3] = {nullptr, nullptr, nullptr};  // exp(-2 pi i m / N[axis]), m < N[axis]
 };
+
+// true unless DISORDER_GENERIC_FFT=1 forces the generic shared-memory kernels
+bool dis_use_fast();
 
 // ---------------------------------------------------------------- line pass
 enum { P_ZERO = 0, P_A = 1, P_B = 2, P_ONE = 3, P_DK = 4 };
@@ -97,6 +101,7 @@ struct LinePassArgs {
   TabRef A, B, T;
   int c00, c01, c10, c11;
   const float* kG;  // device kGrid along the axis (P_DK)
+  const float2* tw;  // device twiddle table of the axis
   FFTPlan plan;
 };
 

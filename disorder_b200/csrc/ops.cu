@@ -24,6 +24,7 @@ LinePassArgs base_args(const disorder_plan_s* plan, int axis, int n_slots) {
   a.in0_s = a.in1_s = a.out0_s = a.out1_s = 0;
   a.c00 = a.c01 = a.c10 = a.c11 = P_ZERO;
   a.kG = plan->d_kG[axis];
+  a.tw = plan->d_tw[axis];
   a.plan = plan->fft[axis];
   return a;
 }

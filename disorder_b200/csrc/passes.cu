@@ -3,7 +3,9 @@
 // memory, FFT, multiply by phase factors (and combine up to two inputs),
 // inverse FFT, store. One HBM read and one write of the volume per pass.
 #include <algorithm>
+#include <cstdlib>
 
+#include "fastpass.h"
 #include "internal.h"
 
 namespace {
@@ -223,9 +225,24 @@ size_t tiles_for(const int* N, int axis, int L) {
 
 }  // namespace
 
+bool dis_use_fast() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("DISORDER_GENERIC_FFT");
+    v = (e && e[0] == '1') ? 0 : 1;
+  }
+  return v == 1;
+}
+
 int dis_line_pass(disorder_ctx_s* ctx, LinePassArgs a) {
   const int n = a.N[a.axis];
   if (a.plan.n != n) return dis_set_error(ctx, DISORDER_BAD_ARG, "line pass: plan size %d != axis size %d", a.plan.n, n);
+  if (a.n_slots == 0) return DISORDER_OK;
+  if (dis_use_fast() && a.tw && dis_fast_line(a, a.tw, ctx->stream)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   const bool two = (a.in1 != nullptr) || (a.out1 != nullptr);
   const int nbuf = (two ? 4 : 2) + (a.accumulate ? 1 : 0);
   a.L = pick_L(n, nbuf, 0);

@@ -1,0 +1,151 @@
+"""Aligned reconstruction driver (the caller of the hot path).
+
+Follows the level / outer-iteration structure of Reconstruction/solveXT.m:
+coil compression (:61), resolution pyramid (pyramidPlan, :38), per level the
+Fourier-cropped image, coils and samples (downsampleOperators, :333-342),
+then outer iterations of CGsolver (:431) and LMsolver (:507) with the
+reference's motion-convergence resets (:379-388) and, once the motion has
+converged or at the last level, a final CGsolver to the energy tolerance
+(:414-425, nIt=300, 'Energy', tolerSolve). Outlier weighting, Haar binning of
+motion states (compressMotion), NIfTI output and the Gibbs/B-spline filters
+of the reference driver are not part of this path.
+"""
+
+import math
+import time
+
+import numpy as np
+
+from . import api
+
+
+def pyramidPlan(voxSiz, resolMax=4.0, NWend=1, accel=(1, 0)):
+    """Methods/pyramidPlan.m:19-33. Returns (resPyr, L, estT, resIso)."""
+    voxSiz = np.asarray(voxSiz, float)
+    Lr = int(round(math.log2(max(resolMax / voxSiz.min(), 1)))) + 1
+    resPyr = 1.0 / np.flip(2.0 ** np.arange(Lr))
+    L = Lr + int(round(math.log2(NWend)))
+    resPyr = np.concatenate([resPyr, np.ones(L - Lr)])
+    estT = np.ones(L, int)
+    estT[max(L - accel[0], 0):L] = 0
+    resIso = math.sqrt(2) * (np.prod(voxSiz) ** (1 / 3)) / resPyr
+    L = max(L - accel[1], 1)
+    return resPyr[:L], L, estT[:L], resIso[:L]
+
+
+def _signed(j, n):
+    return ((j + n // 2) % n) - n // 2
+
+
+def level_sampling(H, n_states, NYres):
+    """Crop the DC-first shot map H to the central NYres frequencies (the
+    k-space crop of resampling(A, NYres, 1), Methods/downsampleOperators.m:53)
+    and list the level's samples as buildHarmonicSampling does. Returns (ky,
+    kz, nEc, mSt, src) with src the row of every level sample in the
+    full-resolution sample array."""
+    N1, N2 = H.shape
+    f1 = np.array([_signed(j, NYres[0]) % N1 for j in range(NYres[0])])
+    f2 = np.array([_signed(j, NYres[1]) % N2 for j in range(NYres[1])])
+    Hres = H[np.ix_(f1, f2)]
+    full_lin = f1[:, None] + N1 * f2[None, :]
+    Hf = Hres.reshape(-1, order="F")
+    Lf = full_lin.reshape(-1, order="F")
+    idx, seg = [], []
+    for s in range(1, n_states + 2):
+        ind = np.flatnonzero(Hf == (s % (n_states + 1)))
+        idx.append(ind)
+        seg.append(np.full(len(ind), s - 1, np.int32))
+    lin = np.concatenate(idx)
+    ky, kz = np.unravel_index(lin, Hres.shape, order="F")
+    nEc = np.concatenate([[0], np.cumsum([len(i) for i in idx])]).astype(np.int64)
+    # rows of the full-resolution sample array: its samples are the grid points
+    # ordered by shot in the same way (H at full size)
+    Hfull = H.reshape(-1, order="F")
+    full_order = np.concatenate([np.flatnonzero(Hfull == (s % (n_states + 1))) for s in range(1, n_states + 2)])
+    row_of = np.empty(H.size, np.int64)
+    row_of[full_order] = np.arange(full_order.size)
+    return ky.astype(np.int32), kz.astype(np.int32), nEc, np.concatenate(seg), row_of[Lf[lin]]
+
+
+class ReconLog:
+    def __init__(self):
+        self.events = []
+        self.t0 = time.perf_counter()
+
+    def add(self, **kw):
+        kw["t"] = time.perf_counter() - self.t0
+        self.events.append(kw)
+
+
+def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), perc=16, resolMax=4.0,
+                           nExtern=20, winit=1e-3, traLimXT=(0.05, 0.02), redFOV=1.0 / 3, echoesMin=4,
+                           tolerSolve=1e-3, log=None):
+    """Motion-corrected reconstruction of one scan on the GPU.
+
+    S: coil maps (N1,N2,N3,C) device array; y: samples (Ns,N3,C) device array
+    on the full k-space grid, ordered by shot as sample_lists(H) orders them
+    (unitary DFT along the phase encodes, image space along the readout); H:
+    (N1,N2) shot map, 1-based, DC first. perc: coil compression (count if >= 1,
+    energy share if < 1). Returns (x device volume, T (n_states, 6), log).
+    """
+    log = log if log is not None else ReconLog()
+    N = tuple(int(n) for n in N)
+    # coil compression (solveXT.m:61)
+    Sc, yc, Ck, _, _ = api.compressCoils(S, perc, y, ctx=ctx)
+    log.add(step="compress", coils=Ck)
+    resPyr, L, estT, resIso = pyramidPlan(voxSiz, resolMax, 1, (1, 0))
+    ky_full = None
+    x = ctx.empty(N)
+    ctx.check(ctx.lib.disorder_memset(ctx.h, x.ptr, 0, x.nbytes))
+    T = np.zeros((n_states, 6), np.float32)
+    E = None
+    for l in range(L):
+        NXres = tuple(int(math.ceil(n * resPyr[l])) for n in N)
+        # level operators (downsampleOperators, solveXT.m:333-342)
+        xRes = api.resampling(x, NXres, ctx=ctx)
+        SRes = api.resampling(Sc, NXres, ctx=ctx)
+        ky, kz, nEc, mSt, src = level_sampling(H, n_states, NXres[:2])
+        scale = math.sqrt(NXres[0] / N[0] * NXres[1] / N[1])
+        ysel = api.gather_samples(yc, src, scale, ctx=ctx)
+        yRes = api.resampling(ysel, (len(src), NXres[2], Ck), ctx=ctx) if NXres[2] != N[2] else ysel
+        cent = [math.ceil((n + 1) / 2.0) for n in NXres]
+        grids = api.generateTransformGrids(N, NXres, cent, sh=1)
+        Se = api.precondition_weights(SRes, 1e-9, ctx=ctx)
+        # readout region for motion estimation and energy (solveXT.m:345-346)
+        nF = np.arange(0, int(math.floor((1 - redFOV) * NXres[2])))
+        Mbe = np.zeros(NXres[2], np.float32)
+        Mbe[nF] = 1
+        Mbe_d = ctx.upload(Mbe)
+        nSa = np.diff(nEc)[:n_states]
+        cT0 = np.zeros(n_states, bool)
+        if estT[l]:
+            cT0[nSa < echoesMin] = True
+        E = api.Struct(Tr=T, NMs=n_states, NSe=n_states + 1, Sf=SRes, grids=grids, ky=ky, kz=kz, nEc=nEc,
+                       mSt=mSt, w=np.full(n_states, winit, np.float32), cT=cT0.copy(), winit=winit,
+                       tL=list(np.asarray(traLimXT) * resIso[l]), nF=nF)
+        EH = api.Struct(Mbe=Mbe_d)
+        A = api.Struct(Se=Se)
+        est = bool(estT[l])
+        nReset, cont = 0, 0
+        for n in range(nExtern):
+            if nReset == 0 or cont % nReset == 0 or np.all(E.cT):  # solveXT.m:379-384
+                nReset += 1
+                cont = 0
+                E.cT = cT0.copy()
+            cont += 1
+            if est:
+                nX, tolType, tol = 1, "RelativeResidual2Error", 0.0  # nIt(2)=1 at motion levels
+            else:
+                nX, tolType, tol = 300, "Energy", tolerSolve
+            xRes, EnX, nn = api.CGsolver(yRes, E, EH, A, None, None, xRes, nX, tolType, tol, ctx=ctx)
+            log.add(step="cg", level=l, it=n, iters=nn, tolType=tolType)
+            if not est:
+                break
+            E = api.LMsolver(yRes, E, xRes, ctx=ctx)
+            T = E.Tr
+            log.add(step="lm", level=l, it=n, unconverged=int(np.sum(~E.cT)),
+                    energy=float(np.sum(E.En)))
+            if np.all(E.cT):  # weak convergence (solveXT.m:530-534)
+                est = False
+        x = api.resampling(xRes, N, ctx=ctx)
+    return x, T, log

@@ -121,11 +121,15 @@ def motion(n_shots, rot_deg, trans_vox, rng):
 
 
 def snr_to_sigma(snr_db, x_gt, S):
-    """Simulation/SNRToLevels.m:23-33."""
+    """Simulation/SNRToLevels.m:23-33, for the unitary encoding of the aligned
+    reconstruction. The reference divides the noise amplification by
+    numel(xGT) (:31) because its simulation encoder applies the unnormalised
+    DFT; with the unitary DFT of encode.m (build1DFTM(N,1)) the same image
+    SNR needs that factor left out, i.e. sigma is the reference's divided by
+    sqrt(numel(xGT))."""
     meanS = np.mean(np.abs(x_gt) ** 2)
     meanN = meanS / (10 ** (snr_db / 10))
-    P = 1.0 / (np.sum(np.abs(S) ** 2, axis=3) + 1e-3)
-    P = np.mean(P) / x_gt.size
+    P = np.mean(1.0 / (np.sum(np.abs(S) ** 2, axis=3) + 1e-3))
     return float(np.sqrt(meanN / (2 * P)))
 
 

@@ -56,6 +56,8 @@ int disorder_malloc(disorder_ctx ctx, size_t bytes, void** dptr);
 int disorder_free(disorder_ctx ctx, void* dptr);
 int disorder_memcpy_h2d(disorder_ctx ctx, void* dst, const void* src, size_t bytes);
 int disorder_memcpy_d2h(disorder_ctx ctx, void* dst, const void* src, size_t bytes);
+int disorder_memcpy_d2d(disorder_ctx ctx, void* dst, const void* src, size_t bytes);
+int disorder_memset(disorder_ctx ctx, void* dst, int value, size_t bytes);
 /* number of kernels this context has launched since creation */
 int64_t disorder_kernel_launches(disorder_ctx ctx);
 /* CUDA-event timing on the context's stream (no reference counterpart):
@@ -152,6 +154,36 @@ int disorder_lm_step(disorder_ctx ctx, disorder_plan plan, const void* y, const 
                      int32_t n_coils, const void* x, float* T, float* w, uint8_t* cT,
                      float winit, const float* tL, int32_t n3_lo, int32_t n3_hi, double* En,
                      double* EnPrev);
+
+/* ---- data preparation ----
+ * x=resampling(x,Nres) for image-space complex data (Methods/resampling.m:45-94,
+ * fo=0, no mirroring): per changed dim, DFT/Nin, centred crop or zero-pad,
+ * inverse DFT*Nout. x, out: device, n_vols volumes of Nin / Nout. */
+int disorder_resample(disorder_ctx ctx, const void* x, const int32_t* Nin, int32_t n_vols,
+                      const int32_t* Nout, void* out);
+
+/* Rows of a sample array picked for a pyramid level (the k-space crop of
+ * Methods/downsampleOperators.m:53,67 on per-sample data):
+ * y_out[i + n_out*r] = scale * y_in[idx[i] + n_in*r], r < rows (readout x coils).
+ * idx: device int32 n_out. */
+int disorder_gather_samples(disorder_ctx ctx, const void* y_in, int64_t n_in, int64_t rows,
+                            const int32_t* idx, int64_t n_out, float scale, void* y_out);
+
+/* A.Se = 1 ./ (sum_c |S_c|^2 + reg) (Reconstruction/solveXT.m:231-233,406-408):
+ * Sf device V x C, out device real V. */
+int disorder_precondition_weights(disorder_ctx ctx, const void* Sf, int32_t n_coils, int64_t V,
+                                  float reg, float* out);
+
+/* [S,y,C,D,U]=compressCoils(S,perc,y) (Methods/compressCoils.m:76-118, the
+ * branch for equal coil and data grids): Gram matrix on the device, Hermitian
+ * eigendecomposition on the host, compression on the device.
+ * S: device V x C_in; y: device n_y x C_in or NULL; perc < 1: energy share,
+ * >= 1: coil count; C_max > 0 caps the count. S_out (V x C_in capacity),
+ * y_out (n_y x C_in capacity): device. C_out: host. D (C_in) and U
+ * (C_in x C_in complex, interleaved, column-major): host or NULL. */
+int disorder_compress_coils(disorder_ctx ctx, const void* S, int32_t C_in, int64_t V, const void* y,
+                            int64_t n_y, double perc, int32_t C_max, void* S_out, void* y_out,
+                            int32_t* C_out, double* D, double* U);
 
 #ifdef __cplusplus
 }

@@ -254,7 +254,9 @@ def test_lm_step(ctx):
     Eol = Eo.copy(**common)
     for it in range(3):
         Edl = db.LMsolver(y.astype(np.complex64), Edl, sc.x_gt, ctx=ctx)
-        Eol = osol.LMsolver(y, Eol, sc.x_gt.astype(np.complex128))
+        # the reference returns E with Sf cropped to nF; solveXT re-sets E.Sf
+        # before every call (solveXT.m:498-503), so do the same here
+        Eol = osol.LMsolver(y, Eol.copy(Sf=Eo.Sf), sc.x_gt.astype(np.complex128))
         assert np.array_equal(Edl.cT, Eol.cT), it
         assert rel(Edl.Tr, Eol.Tr) < TOL_SOLVER, (it, Edl.Tr, Eol.Tr)
         assert rel(Edl.w, Eol.w) < 1e-6
