@@ -430,6 +430,7 @@ int disorder_encodedecode(disorder_ctx ctx, disorder_plan plan, const void* x, c
   sp.T_n = plan->n_mot;
   sp.segs = all_segs(plan);
   sp.wmap = wmap;
+  sp.We = We;
   return dis_encodedecode_segments(ctx, plan, sp, (float2*)out);
 }
 

@@ -1,17 +1,18 @@
 // Encoding operators over the segments of a plan
 // (Reconstruction/encode.m, decode.m, encodedecode.m; hot fields only).
-// Segments are processed in chunks sized to the workspace budget; within a
-// chunk every kernel covers all of the chunk's segments and coils.
+// The coil stage runs as the fused plane kernel (plane.cuh) when its shared
+// memory fits (C x samples-per-segment); otherwise as three passes through
+// per-coil buffers (coil.cu). Segments are processed in chunks sized to the
+// workspace budget.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <vector>
 
-#include "internal.h"
 #include "encoding.h"
-
-int dis_sum_slots(disorder_ctx_s* ctx, const float2* u, long long V, int n_slots, float2* out, float beta);
-int dis_broadcast(disorder_ctx_s* ctx, const float2* x, long long V, int n_slots, float2* out);
+#include "fastpass.h"
+#include "internal.h"
+#include "plane.cuh"
 
 size_t dis_budget_bytes() {
   const char* e = std::getenv("DISORDER_WORKSPACE_GB");
@@ -57,7 +58,7 @@ int dis_upload_ints(disorder_ctx_s* ctx, Workspace* ws, const std::vector<int>& 
   return DISORDER_OK;
 }
 
-// per-slot coil-stage bytes
+// per-slot coil-stage bytes of the three-pass path
 static size_t coil_slot_bytes(const disorder_plan_s* plan, int C, int N3c) {
   return (size_t)C * plan->N[0] * plan->N[1] * N3c * sizeof(float2);
 }
@@ -69,6 +70,134 @@ int dis_chunk_slots(const disorder_plan_s* plan, int C, int N3c, size_t extra_pe
   return std::max(1, std::min(ch, n_total));
 }
 
+// ---------------------------------------------------------------- plane path
+static int max_samples(const disorder_plan_s* plan, const std::vector<int>& segs) {
+  long long m = 0;
+  for (int s : segs) m = std::max(m, plan->seg_off[s + 1] - plan->seg_off[s]);
+  return (int)m;
+}
+
+// The fused plane kernel trades HBM traffic for arithmetic (the restricted
+// DFT costs Ns*N2 MACs per coil-plane) and holds one CTA per SM at 256x256;
+// on B200 the three-pass path is faster at the benchmark sizes, so the plane
+// kernel is used only when DISORDER_PLANE=1.
+static bool plane_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("DISORDER_PLANE");
+    v = (e && e[0] == '1') ? 1 : 0;
+  }
+  return v == 1;
+}
+
+bool dis_plane_usable(const disorder_plan_s* plan, int C, const std::vector<int>& segs) {
+  if (!dis_use_fast() || !plane_enabled()) return false;
+  const size_t b = dis_plane_smem(plan->N[0], plan->N[1], C, std::max(1, max_samples(plan, segs)));
+  return b <= 225 * 1024;
+}
+
+static int plane_run(disorder_ctx_s* ctx, const disorder_plan_s* plan, int mode, const float2* z, long long Vz,
+                     float2* u, long long Vu, const float2* Sf, int C, int n3_lo, int N3c, const int* d_seg, int n_slots,
+                     int max_ns, float2* y, const float2* ymeas, long long ld, int y_n3off, int y_N3,
+                     const float* We, const float* Mb) {
+  if (n_slots == 0 || N3c == 0) return DISORDER_OK;
+  const long long pl3 = (long long)n3_lo * plan->N[0] * plan->N[1];
+  pl::PlaneArgs a;
+  a.N1 = plan->N[0];
+  a.N2 = plan->N[1];
+  a.N3c = N3c;
+  a.Vz = Vz;
+  a.Vu = Vu;
+  a.z = z + pl3;
+  a.u = u ? u + pl3 : nullptr;
+  a.Sf = Sf + pl3;
+  a.Sc = plan->V;
+  a.C = C;
+  a.slot_seg = d_seg;
+  a.seg_off = plan->d_seg_off;
+  a.ky = plan->d_ky;
+  a.kz = plan->d_kz;
+  a.rowptr = plan->d_rowptr;
+  a.perm = plan->d_perm;
+  a.y = y;
+  a.ymeas = ymeas;
+  a.ld = ld;
+  a.y_n3off = y_n3off;
+  a.y_N3 = y_N3;
+  a.We = We;
+  a.Mb = Mb;
+  const double n12 = (double)plan->N[0] * plan->N[1];
+  a.scale_f = (float)(1.0 / std::sqrt(n12));
+  a.scale_a = (float)(mode == pl::ENCDEC ? 1.0 / n12 : 1.0 / std::sqrt(n12));
+  a.max_ns = std::max(1, max_ns);
+  if (!dis_fast_plane(plan->N[0], mode, a, plan->d_tw[0], plan->d_tw[1], n_slots, ctx->stream))
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "plane kernel unavailable for N1=%d", plan->N[0]);
+  dis_count(ctx);
+  DIS_CUDA_TRY(cudaGetLastError());
+  return DISORDER_OK;
+}
+
+// forward transform of the chunk's motion segments into Z, untransformed
+// copies for the outer segments; returns the state volumes and their stride
+static int states_of(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* x, const float* T, int T_n,
+                     bool motion, const std::vector<int>& segs, Workspace* w, const float2** z, long long* Vz,
+                     float2** Zout, int* n_mot) {
+  const long long V = plan->V;
+  const int n = (int)segs.size();
+  *n_mot = 0;
+  if (!motion) {
+    *z = x;
+    *Vz = 0;
+    if (Zout) *Zout = nullptr;
+    return DISORDER_OK;
+  }
+  float2* Z = w->take<float2>((size_t)n * V);
+  if (!Z) return dis_set_error(ctx, DISORDER_OOM, "workspace too small");
+  std::vector<int> mot;
+  for (int s : segs)
+    if (s < plan->n_mot) mot.push_back(s);
+  const int nm = (int)mot.size();  // motion segments come first
+  if (nm) {
+    std::vector<SlotParams> prm;
+    dis_slot_params(T, T_n, mot.data(), nm, 1, &prm);
+    Tables tb;
+    DIS_TRY(dis_build_tables(ctx, plan, prm, false, w, &tb));
+    DIS_TRY(dis_forward_transform(ctx, plan, x, 0, Z, tb, 1, nullptr));
+  }
+  if (n > nm) DIS_TRY(dis_broadcast(ctx, x, V, n - nm, Z + (long long)nm * V));
+  *z = Z;
+  *Vz = V;
+  if (Zout) *Zout = Z;
+  *n_mot = nm;
+  return DISORDER_OK;
+}
+
+// inverse transform of the motion slots of U summed into out, outer slots added
+static int sum_back(disorder_ctx_s* ctx, const disorder_plan_s* plan, float2* U, const float* T, int T_n,
+                    const std::vector<int>& segs, int nm, Workspace* w, float2* out, bool* first) {
+  const long long V = plan->V;
+  const int n = (int)segs.size();
+  if (nm) {
+    std::vector<SlotParams> prm;
+    dis_slot_params(T, T_n, segs.data(), nm, 0, &prm);
+    Tables tb;
+    DIS_TRY(dis_build_tables(ctx, plan, prm, false, w, &tb));
+    DIS_TRY(dis_inverse_transform(ctx, plan, U, tb, 1, out, *first ? 0.f : 1.f));
+    *first = false;
+  }
+  if (n > nm) {
+    DIS_TRY(dis_sum_slots(ctx, U + (long long)nm * V, V, n - nm, out, *first ? 0.f : 1.f));
+    *first = false;
+  }
+  return DISORDER_OK;
+}
+
+static int plane_chunk(const disorder_plan_s* plan, int nsg, size_t per_slot) {
+  const size_t per = per_slot + dis_table_bytes(plan, 1, false);
+  const int ch = (int)std::max<size_t>(1, dis_budget_bytes() / std::max<size_t>(per, 1));
+  return std::max(1, std::min(ch, nsg));
+}
+
 // ---------------------------------------------------------------- encode
 int dis_encode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const EncodeSpec& sp, float2* y,
                         const float2* y_meas) {
@@ -76,6 +205,26 @@ int dis_encode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
   const int nsg = (int)sp.segs.size();
   if (nsg == 0) return DISORDER_OK;
   const bool motion = dis_any_motion(sp.T, sp.T_n);
+  if (dis_plane_usable(plan, sp.C, sp.segs)) {
+    const int ch = motion ? plane_chunk(plan, nsg, V * sizeof(float2)) : nsg;
+    Workspace ws;
+    DIS_TRY(dis_workspace(ctx, (motion ? (size_t)ch * V * sizeof(float2) : 0) + dis_table_bytes(plan, ch, false) +
+                                   (1 << 20), &ws));
+    for (int c0 = 0; c0 < nsg; c0 += ch) {
+      const int n = std::min(ch, nsg - c0);
+      Workspace w = ws;
+      std::vector<int> segs(sp.segs.begin() + c0, sp.segs.begin() + c0 + n);
+      int* d_seg = nullptr;
+      DIS_TRY(dis_upload_ints(ctx, &w, segs, &d_seg));
+      const float2* z;
+      long long Vz;
+      int nm;
+      DIS_TRY(states_of(ctx, plan, sp.x, sp.T, sp.T_n, motion, segs, &w, &z, &Vz, nullptr, &nm));
+      DIS_TRY(plane_run(ctx, plan, pl::ENCODE, z, Vz, nullptr, 0, sp.Sf, sp.C, sp.n3_lo, sp.N3c, d_seg, n,
+                        max_samples(plan, segs), y, y_meas, sp.y_ld, sp.y_n3off, sp.y_N3, nullptr, nullptr));
+    }
+    return DISORDER_OK;
+  }
   const int ch = dis_chunk_slots(plan, sp.C, sp.N3c, motion ? V * sizeof(float2) : 0, nsg);
   const size_t need = (size_t)ch * coil_slot_bytes(plan, sp.C, sp.N3c) + (motion ? (size_t)ch * V * sizeof(float2) : 0) +
                       dis_table_bytes(plan, ch, false) + 4096 * 4;
@@ -89,26 +238,10 @@ int dis_encode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
     DIS_TRY(dis_upload_ints(ctx, &w, segs, &d_seg));
     float2* A = w.take<float2>((size_t)n * sp.C * plan->N[0] * plan->N[1] * sp.N3c);
     if (!A) return dis_set_error(ctx, DISORDER_OOM, "encode: workspace too small");
-    const float2* z = sp.x;
-    long long Vz = 0;
-    if (motion) {
-      float2* Z = w.take<float2>((size_t)n * V);
-      if (!Z) return dis_set_error(ctx, DISORDER_OOM, "encode: workspace too small");
-      std::vector<int> mot;
-      for (int j = 0; j < n; ++j)
-        if (segs[j] < plan->n_mot) mot.push_back(segs[j]);
-      const int nm = (int)mot.size();  // motion segments come first in a chunk
-      if (nm) {
-        std::vector<SlotParams> prm;
-        dis_slot_params(sp.T, sp.T_n, mot.data(), nm, 1, &prm);
-        Tables tb;
-        DIS_TRY(dis_build_tables(ctx, plan, prm, false, &w, &tb));
-        DIS_TRY(dis_forward_transform(ctx, plan, sp.x, 0, Z, tb, 1, nullptr));
-      }
-      if (n > nm) DIS_TRY(dis_broadcast(ctx, sp.x, V, n - nm, Z + (long long)nm * V));
-      z = Z;
-      Vz = V;
-    }
+    const float2* z;
+    long long Vz;
+    int nm;
+    DIS_TRY(states_of(ctx, plan, sp.x, sp.T, sp.T_n, motion, segs, &w, &z, &Vz, nullptr, &nm));
     CoilArgs ca = coil_args(plan, sp.Sf, sp.C, sp.n3_lo, sp.N3c, Vz, n, d_seg);
     DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, z + (long long)sp.n3_lo * plan->N[0] * plan->N[1], A));
     const float scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
@@ -119,8 +252,13 @@ int dis_encode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
 
 // coil stage only, for per-slot volumes vols (stride V) whose segments are segs
 int dis_encode_volumes(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* vols, const int* d_segs,
-                       int n, const float2* Sf, int C, int n3_lo, int N3c, float2* A, float2* y, long long y_ld,
-                       int y_n3off, int y_N3, const float2* y_meas) {
+                       const std::vector<int>& segs, const float2* Sf, int C, int n3_lo, int N3c, float2* A,
+                       float2* y, long long y_ld, int y_n3off, int y_N3, const float2* y_meas) {
+  const int n = (int)segs.size();
+  if (dis_plane_usable(plan, C, segs))
+    return plane_run(ctx, plan, pl::ENCODE, vols, plan->V, nullptr, 0, Sf, C, n3_lo, N3c, d_segs, n,
+                     max_samples(plan, segs), y, y_meas, y_ld, y_n3off, y_N3, nullptr, nullptr);
+  if (!A) return dis_set_error(ctx, DISORDER_OOM, "encode_volumes: no coil buffer");
   CoilArgs ca = coil_args(plan, Sf, C, n3_lo, N3c, plan->V, n, d_segs);
   DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, vols + (long long)n3_lo * plan->N[0] * plan->N[1], A));
   const float scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
@@ -137,12 +275,34 @@ int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
   }
   const bool motion = dis_any_motion(sp.T, sp.T_n);
   const int N3 = plan->N[2];
+  bool first = true;
+  if (dis_plane_usable(plan, sp.C, sp.segs)) {
+    const int ch = plane_chunk(plan, nsg, V * sizeof(float2));
+    Workspace ws;
+    DIS_TRY(dis_workspace(ctx, (size_t)ch * V * sizeof(float2) + dis_table_bytes(plan, ch, false) + (1 << 20), &ws));
+    for (int c0 = 0; c0 < nsg; c0 += ch) {
+      const int n = std::min(ch, nsg - c0);
+      Workspace w = ws;
+      std::vector<int> segs(sp.segs.begin() + c0, sp.segs.begin() + c0 + n);
+      int* d_seg = nullptr;
+      DIS_TRY(dis_upload_ints(ctx, &w, segs, &d_seg));
+      float2* U = w.take<float2>((size_t)n * V);
+      if (!U) return dis_set_error(ctx, DISORDER_OOM, "decode: workspace too small");
+      DIS_TRY(plane_run(ctx, plan, pl::DECODE, U, V, U, V, sp.Sf, sp.C, 0, N3, d_seg, n, max_samples(plan, segs),
+                        const_cast<float2*>(sp.y), nullptr, plan->n_samples, 0, N3, sp.We, sp.Mb));
+      int nm = 0;
+      if (motion)
+        for (int s : segs)
+          if (s < plan->n_mot) ++nm;
+      DIS_TRY(sum_back(ctx, plan, U, sp.T, sp.T_n, segs, nm, &w, out, &first));
+    }
+    return DISORDER_OK;
+  }
   const int ch = dis_chunk_slots(plan, sp.C, N3, V * sizeof(float2), nsg);
   const size_t need = (size_t)ch * (coil_slot_bytes(plan, sp.C, N3) + V * sizeof(float2)) +
                       dis_table_bytes(plan, ch, false) + 4096 * 4;
   Workspace ws;
   DIS_TRY(dis_workspace(ctx, need, &ws));
-  bool first = true;
   for (int c0 = 0; c0 < nsg; c0 += ch) {
     const int n = std::min(ch, nsg - c0);
     Workspace w = ws;
@@ -158,20 +318,9 @@ int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
     DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
     int nm = 0;
     if (motion)
-      for (int j = 0; j < n; ++j)
-        if (segs[j] < plan->n_mot) ++nm;
-    if (nm) {
-      std::vector<SlotParams> prm;
-      dis_slot_params(sp.T, sp.T_n, segs.data(), nm, 0, &prm);
-      Tables tb;
-      DIS_TRY(dis_build_tables(ctx, plan, prm, false, &w, &tb));
-      DIS_TRY(dis_inverse_transform(ctx, plan, U, tb, 1, out, first ? 0.f : 1.f));
-      first = false;
-    }
-    if (n > nm) {
-      DIS_TRY(dis_sum_slots(ctx, U + (long long)nm * V, V, n - nm, out, first ? 0.f : 1.f));
-      first = false;
-    }
+      for (int s : segs)
+        if (s < plan->n_mot) ++nm;
+    DIS_TRY(sum_back(ctx, plan, U, sp.T, sp.T_n, segs, nm, &w, out, &first));
   }
   return DISORDER_OK;
 }
@@ -187,12 +336,50 @@ int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, 
   }
   const bool motion = dis_any_motion(sp.T, sp.T_n);
   const int N3 = plan->N[2];
+  bool first = true;
+  if (dis_plane_usable(plan, sp.C, sp.segs)) {
+    const int ch = plane_chunk(plan, nsg, V * sizeof(float2));
+    Workspace ws;
+    DIS_TRY(dis_workspace(ctx, (size_t)ch * V * sizeof(float2) + 2 * dis_table_bytes(plan, ch, false) + (1 << 20),
+                          &ws));
+    for (int c0 = 0; c0 < nsg; c0 += ch) {
+      const int n = std::min(ch, nsg - c0);
+      Workspace w = ws;
+      std::vector<int> segs(sp.segs.begin() + c0, sp.segs.begin() + c0 + n);
+      int* d_seg = nullptr;
+      DIS_TRY(dis_upload_ints(ctx, &w, segs, &d_seg));
+      float2* U = w.take<float2>((size_t)n * V);
+      if (!U) return dis_set_error(ctx, DISORDER_OOM, "encodedecode: workspace too small");
+      int nm = 0;
+      if (motion) {
+        std::vector<int> mot;
+        for (int s : segs)
+          if (s < plan->n_mot) mot.push_back(s);
+        nm = (int)mot.size();
+        if (nm) {
+          std::vector<SlotParams> prm;
+          dis_slot_params(sp.T, sp.T_n, mot.data(), nm, 1, &prm);
+          Tables tb;
+          DIS_TRY(dis_build_tables(ctx, plan, prm, false, &w, &tb));
+          DIS_TRY(dis_forward_transform(ctx, plan, sp.x, 0, U, tb, 1, nullptr));
+        }
+        if (n > nm) DIS_TRY(dis_broadcast(ctx, sp.x, V, n - nm, U + (long long)nm * V));
+        // the plane kernel reads each plane of U fully before writing it back
+        DIS_TRY(plane_run(ctx, plan, pl::ENCDEC, U, V, U, V, sp.Sf, sp.C, 0, N3, d_seg, n, max_samples(plan, segs),
+                          nullptr, nullptr, plan->n_samples, 0, N3, sp.We, nullptr));
+      } else {
+        DIS_TRY(plane_run(ctx, plan, pl::ENCDEC, sp.x, 0, U, V, sp.Sf, sp.C, 0, N3, d_seg, n, max_samples(plan, segs),
+                          nullptr, nullptr, plan->n_samples, 0, N3, sp.We, nullptr));
+      }
+      DIS_TRY(sum_back(ctx, plan, U, sp.T, sp.T_n, segs, nm, &w, out, &first));
+    }
+    return DISORDER_OK;
+  }
   const int ch = dis_chunk_slots(plan, sp.C, N3, V * sizeof(float2), nsg);
   const size_t need = (size_t)ch * (coil_slot_bytes(plan, sp.C, N3) + V * sizeof(float2)) +
                       2 * dis_table_bytes(plan, ch, false) + 4096 * 4;
   Workspace ws;
   DIS_TRY(dis_workspace(ctx, need, &ws));
-  bool first = true;
   for (int c0 = 0; c0 < nsg; c0 += ch) {
     const int n = std::min(ch, nsg - c0);
     Workspace w = ws;
@@ -200,46 +387,24 @@ int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, 
     int* d_seg = nullptr;
     DIS_TRY(dis_upload_ints(ctx, &w, segs, &d_seg));
     float2* A = w.take<float2>((size_t)n * sp.C * V);
-    float2* Z = w.take<float2>((size_t)n * V);
-    if (!A || !Z) return dis_set_error(ctx, DISORDER_OOM, "encodedecode: workspace too small");
-    int nm = 0;
-    if (motion)
-      for (int j = 0; j < n; ++j)
-        if (segs[j] < plan->n_mot) ++nm;
-    Tables tb;
-    if (nm) {
-      std::vector<SlotParams> prm;
-      dis_slot_params(sp.T, sp.T_n, segs.data(), nm, 1, &prm);
-      DIS_TRY(dis_build_tables(ctx, plan, prm, false, &w, &tb));
-      DIS_TRY(dis_forward_transform(ctx, plan, sp.x, 0, Z, tb, 1, nullptr));
-    }
-    const float2* z = Z;
-    long long Vz = V;
-    if (!motion) {
-      z = sp.x;
-      Vz = 0;
-    } else if (n > nm) {
-      DIS_TRY(dis_broadcast(ctx, sp.x, V, n - nm, Z + (long long)nm * V));
+    if (!A) return dis_set_error(ctx, DISORDER_OOM, "encodedecode: workspace too small");
+    const float2* z;
+    long long Vz;
+    float2* Z = nullptr;
+    int nm;
+    DIS_TRY(states_of(ctx, plan, sp.x, sp.T, sp.T_n, motion, segs, &w, &z, &Vz, &Z, &nm));
+    float2* U = Z;
+    if (!U) {
+      U = w.take<float2>((size_t)n * V);
+      if (!U) return dis_set_error(ctx, DISORDER_OOM, "encodedecode: workspace too small");
     }
     CoilArgs ca = coil_args(plan, sp.Sf, sp.C, 0, N3, Vz, n, d_seg);
     DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, z, A));
     DIS_TRY(dis_coil_fft2_weight(ctx, plan, ca, A, sp.wmap));
     ca.Vz = V;
     const float scale = (float)(1.0 / ((double)plan->N[0] * plan->N[1]));
-    DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, Z, scale));
-    if (nm) {
-      // inverse transform factors (di=0) for the motion slots
-      std::vector<SlotParams> prm;
-      dis_slot_params(sp.T, sp.T_n, segs.data(), nm, 0, &prm);
-      Tables tbi;
-      DIS_TRY(dis_build_tables(ctx, plan, prm, false, &w, &tbi));
-      DIS_TRY(dis_inverse_transform(ctx, plan, Z, tbi, 1, out, first ? 0.f : 1.f));
-      first = false;
-    }
-    if (n > nm) {
-      DIS_TRY(dis_sum_slots(ctx, Z + (long long)nm * V, V, n - nm, out, first ? 0.f : 1.f));
-      first = false;
-    }
+    DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
+    DIS_TRY(sum_back(ctx, plan, U, sp.T, sp.T_n, segs, nm, &w, out, &first));
   }
   return DISORDER_OK;
 }

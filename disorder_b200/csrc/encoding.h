@@ -34,7 +34,8 @@ struct EncodeDecodeSpec {
   const float* T = nullptr;
   int T_n = 0;
   std::vector<int> segs;
-  const float* wmap = nullptr;  // [seg][N2][N1] sample weights of each grid point
+  const float* wmap = nullptr;  // [seg][N2][N1] sample weights of each grid point (three-pass path)
+  const float* We = nullptr;    // per-sample weights (plane path), NULL for 1
 };
 
 size_t dis_budget_bytes();
@@ -45,12 +46,13 @@ int dis_upload_ints(disorder_ctx_s* ctx, Workspace* ws, const std::vector<int>& 
 int dis_encode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const EncodeSpec& sp, float2* y,
                         const float2* y_meas);
 int dis_encode_volumes(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* vols, const int* d_segs,
-                       int n, const float2* Sf, int C, int n3_lo, int N3c, float2* A, float2* y, long long y_ld,
+                       const std::vector<int>& segs, const float2* Sf, int C, int n3_lo, int N3c, float2* A, float2* y, long long y_ld,
                        int y_n3off, int y_N3, const float2* y_meas);
 int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const DecodeSpec& sp, float2* out);
 int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const EncodeDecodeSpec& sp,
                               float2* out);
 int dis_gradient(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* x, long long x_s,
                  const Tables& tb, float2* z, float2* yB, float2* w1, float2* w2, float2* G);
+bool dis_plane_usable(const disorder_plan_s* plan, int C, const std::vector<int>& segs);
 int dis_sum_slots(disorder_ctx_s* ctx, const float2* u, long long V, int n_slots, float2* out, float beta);
 int dis_broadcast(disorder_ctx_s* ctx, const float2* x, long long V, int n_slots, float2* out);

@@ -1,7 +1,11 @@
-// Explicit instantiations of the register-resident line-pass kernels
-// for line lengths 16, 32, 44.
+// Explicit instantiations of the register-resident line-pass and plane
+// kernels for line lengths 16, 32, 44.
 #include "fastpass.cuh"
+#include "plane.cuh"
 
 DIS_FAST_INSTANTIATE(4, 4)  // N = 16
+template struct pl::PlaneLaunch<4, 4>;
 DIS_FAST_INSTANTIATE(8, 4)  // N = 32
+template struct pl::PlaneLaunch<8, 4>;
 DIS_FAST_INSTANTIATE(4, 11)  // N = 44
+template struct pl::PlaneLaunch<4, 11>;

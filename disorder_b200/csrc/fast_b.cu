@@ -1,6 +1,9 @@
-// Explicit instantiations of the register-resident line-pass kernels
-// for line lengths 64, 88.
+// Explicit instantiations of the register-resident line-pass and plane
+// kernels for line lengths 64, 88.
 #include "fastpass.cuh"
+#include "plane.cuh"
 
 DIS_FAST_INSTANTIATE(8, 8)  // N = 64
+template struct pl::PlaneLaunch<8, 8>;
 DIS_FAST_INSTANTIATE(8, 11)  // N = 88
+template struct pl::PlaneLaunch<8, 11>;

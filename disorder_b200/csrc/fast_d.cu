@@ -1,6 +1,9 @@
-// Explicit instantiations of the register-resident line-pass kernels
-// for line lengths 160, 176.
+// Explicit instantiations of the register-resident line-pass and plane
+// kernels for line lengths 160, 176.
 #include "fastpass.cuh"
+#include "plane.cuh"
 
 DIS_FAST_INSTANTIATE(16, 10)  // N = 160
+template struct pl::PlaneLaunch<16, 10>;
 DIS_FAST_INSTANTIATE(16, 11)  // N = 176
+template struct pl::PlaneLaunch<16, 11>;

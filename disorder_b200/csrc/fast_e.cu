@@ -1,6 +1,9 @@
-// Explicit instantiations of the register-resident line-pass kernels
-// for line lengths 192, 256.
+// Explicit instantiations of the register-resident line-pass and plane
+// kernels for line lengths 192, 256.
 #include "fastpass.cuh"
+#include "plane.cuh"
 
 DIS_FAST_INSTANTIATE(16, 12)  // N = 192
+template struct pl::PlaneLaunch<16, 12>;
 DIS_FAST_INSTANTIATE(16, 16)  // N = 256
+template struct pl::PlaneLaunch<16, 16>;

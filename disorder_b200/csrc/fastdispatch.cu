@@ -2,6 +2,7 @@
 // instantiated in fast_[a-e].cu (one translation unit per group of sizes).
 #include "fastpass.cuh"
 #include "fastpass.h"
+#include "plane.cuh"
 
 extern template struct fp::Launch<4, 4>;
 extern template struct fp::Launch<8, 4>;
@@ -14,6 +15,18 @@ extern template struct fp::Launch<16, 10>;
 extern template struct fp::Launch<16, 11>;
 extern template struct fp::Launch<16, 12>;
 extern template struct fp::Launch<16, 16>;
+
+extern template struct pl::PlaneLaunch<4, 4>;
+extern template struct pl::PlaneLaunch<8, 4>;
+extern template struct pl::PlaneLaunch<4, 11>;
+extern template struct pl::PlaneLaunch<8, 8>;
+extern template struct pl::PlaneLaunch<8, 11>;
+extern template struct pl::PlaneLaunch<8, 12>;
+extern template struct pl::PlaneLaunch<16, 8>;
+extern template struct pl::PlaneLaunch<16, 10>;
+extern template struct pl::PlaneLaunch<16, 11>;
+extern template struct pl::PlaneLaunch<16, 12>;
+extern template struct pl::PlaneLaunch<16, 16>;
 
 bool dis_fast_factor(int n, int* F1, int* F2) {
   switch (n) {
@@ -100,5 +113,40 @@ bool dis_fast_axis1(int n, int mode, const CoilArgs& a, float2* A, float2* y, co
     case 192: fp::Launch<16, 12>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
     case 256: fp::Launch<16, 16>::axis1(mode, a, A, y, ymeas, ld, n3off, N3y, scale, wmap, We, Mb, plan, tw, s); return true;
     default: return false;
+  }
+}
+
+bool dis_fast_plane(int n1, int mode, const pl::PlaneArgs& a, const float2* tw1, const float2* tw2, int n_slots,
+                    cudaStream_t s) {
+  switch (n1) {
+    case 16: return pl::PlaneLaunch<4, 4>::run(mode, a, tw1, tw2, n_slots, s);
+    case 32: return pl::PlaneLaunch<8, 4>::run(mode, a, tw1, tw2, n_slots, s);
+    case 44: return pl::PlaneLaunch<4, 11>::run(mode, a, tw1, tw2, n_slots, s);
+    case 64: return pl::PlaneLaunch<8, 8>::run(mode, a, tw1, tw2, n_slots, s);
+    case 88: return pl::PlaneLaunch<8, 11>::run(mode, a, tw1, tw2, n_slots, s);
+    case 96: return pl::PlaneLaunch<8, 12>::run(mode, a, tw1, tw2, n_slots, s);
+    case 128: return pl::PlaneLaunch<16, 8>::run(mode, a, tw1, tw2, n_slots, s);
+    case 160: return pl::PlaneLaunch<16, 10>::run(mode, a, tw1, tw2, n_slots, s);
+    case 176: return pl::PlaneLaunch<16, 11>::run(mode, a, tw1, tw2, n_slots, s);
+    case 192: return pl::PlaneLaunch<16, 12>::run(mode, a, tw1, tw2, n_slots, s);
+    case 256: return pl::PlaneLaunch<16, 16>::run(mode, a, tw1, tw2, n_slots, s);
+    default: return false;
+  }
+}
+
+size_t dis_plane_smem(int n1, int N2, int C, int max_ns) {
+  switch (n1) {
+    case 16: return pl::Layout<4, 4>::bytes(N2, C, max_ns);
+    case 32: return pl::Layout<8, 4>::bytes(N2, C, max_ns);
+    case 44: return pl::Layout<4, 11>::bytes(N2, C, max_ns);
+    case 64: return pl::Layout<8, 8>::bytes(N2, C, max_ns);
+    case 88: return pl::Layout<8, 11>::bytes(N2, C, max_ns);
+    case 96: return pl::Layout<8, 12>::bytes(N2, C, max_ns);
+    case 128: return pl::Layout<16, 8>::bytes(N2, C, max_ns);
+    case 160: return pl::Layout<16, 10>::bytes(N2, C, max_ns);
+    case 176: return pl::Layout<16, 11>::bytes(N2, C, max_ns);
+    case 192: return pl::Layout<16, 12>::bytes(N2, C, max_ns);
+    case 256: return pl::Layout<16, 16>::bytes(N2, C, max_ns);
+    default: return (size_t)-1;
   }
 }

@@ -13,3 +13,12 @@ bool dis_fast_combine(int n, const CoilArgs& a, const float2* A, float2* u, floa
 bool dis_fast_axis1(int n, int mode, const CoilArgs& a, float2* A, float2* y, const float2* ymeas, long long ld,
                     int n3off, int N3y, float scale, const float* wmap, const float* We, const float* Mb,
                     const disorder_plan_s* plan, const float2* tw, cudaStream_t s);
+
+namespace pl {
+struct PlaneArgs;
+}
+// Fused coil stage (plane.cuh). mode: 0 encode, 1 decode, 2 encodedecode.
+// Returns false when N1 has no fast kernel or the shared memory does not fit.
+bool dis_fast_plane(int n1, int mode, const pl::PlaneArgs& a, const float2* tw1, const float2* tw2, int n_slots,
+                    cudaStream_t s);
+size_t dis_plane_smem(int n1, int N2, int C, int max_ns);

@@ -331,6 +331,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   es.T_n = plan->n_mot;
   es.segs = segs;
   es.wmap = wmap;
+  es.We = s.We;
   auto normal_op = [&](const float2* in, float2* out) -> int {
     es.x = in;
     return dis_encodedecode_segments(ctx, plan, es, out);
@@ -553,10 +554,10 @@ int dis_lm_step(disorder_ctx_s* ctx, const disorder_plan_s* plan, const LMSpec& 
     DIS_TRY(dis_build_tables(ctx, plan, prm, true, &w0, &tb));
     DIS_TRY(dis_gradient(ctx, plan, s.x, 0, tb, z, yB, w1, w2, G));
     // r = encode(xT) - y (:72), the derivative encodes (:97-99)
-    DIS_TRY(dis_encode_volumes(ctx, plan, z, d_seg, n, s.Sf, s.C, n3_lo, N3c, A, rbuf, plan->n_samples, n3_lo, N3,
+    DIS_TRY(dis_encode_volumes(ctx, plan, z, d_seg, st, s.Sf, s.C, n3_lo, N3c, A, rbuf, plan->n_samples, n3_lo, N3,
                                s.y));
     for (int g = 0; g < 6; ++g)
-      DIS_TRY(dis_encode_volumes(ctx, plan, G + (long long)g * n * V, d_seg, n, s.Sf, s.C, n3_lo, N3c, A,
+      DIS_TRY(dis_encode_volumes(ctx, plan, G + (long long)g * n * V, d_seg, st, s.Sf, s.C, n3_lo, N3c, A,
                                  gbuf + (long long)g * ny, plan->n_samples, n3_lo, N3, nullptr));
     double* d_out = w0.take<double>((size_t)n * 28);
     if (!d_out) return dis_set_error(ctx, DISORDER_OOM, "LM workspace");
@@ -620,7 +621,7 @@ int dis_lm_step(disorder_ctx_s* ctx, const disorder_plan_s* plan, const LMSpec& 
       Tables tb;
       DIS_TRY(dis_build_tables(ctx, plan, prm, false, &w0, &tb));
       DIS_TRY(dis_forward_transform(ctx, plan, s.x, 0, z, tb, 1, nullptr));
-      DIS_TRY(dis_encode_volumes(ctx, plan, z, d_seg, n, s.Sf, s.C, n3_lo, N3c, A, rbuf, plan->n_samples, n3_lo, N3,
+      DIS_TRY(dis_encode_volumes(ctx, plan, z, d_seg, st, s.Sf, s.C, n3_lo, N3c, A, rbuf, plan->n_samples, n3_lo, N3,
                                  s.y));
       double* d_out = w0.take<double>((size_t)n * 28);
       if (!d_out) return dis_set_error(ctx, DISORDER_OOM, "LM workspace");
