@@ -58,6 +58,7 @@ SIGNATURES = [
     ("disorder_plan_create", C.c_int, [VP, C.POINTER(GridDesc), C.POINTER(SamplingDesc), C.POINTER(VP)]),
     ("disorder_plan_destroy", C.c_int, [VP]),
     ("disorder_sinc_rigid_transform", C.c_int, [VP, VP, VP, I32, FP, I32, I32, I32, I32, VP]),
+    ("disorder_sinc_rigid_transform_static", C.c_int, [VP, VP, VP, I32, FP, I32, I32, I32, VP]),
     ("disorder_sinc_rigid_transform_gradient", C.c_int, [VP, VP, VP, FP, I32, VP, VP]),
     ("disorder_encode", C.c_int, [VP, VP, VP, VP, I32, FP, VP]),
     ("disorder_decode", C.c_int, [VP, VP, VP, VP, I32, FP, VP, VP, VP]),

@@ -140,6 +140,11 @@ void dis_slot_params(const float* T, int n_states, const int* slots, int n_slots
                      std::vector<SlotParams>* out);
 int dis_build_tables(disorder_ctx_s* ctx, const disorder_plan_s* plan, const std::vector<SlotParams>& sp,
                      bool with_grad, Workspace* ws, Tables* tb);
+constexpr int kMaxStaticSlots = 256;
+int dis_build_tables_into(disorder_ctx_s* ctx, const disorder_plan_s* plan, const SlotParams* sp, int ns,
+                          char* base, size_t cap, Tables* tb);
+// per-slot scalars into a caller array (no heap)
+void dis_slot_params_into(const float* T, int n_states, int di, SlotParams* out);
 
 // transform drivers (ops.cu)
 int dis_forward_transform(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* x, long long x_s,

@@ -66,6 +66,25 @@ __global__ void trans_table_kernel(float2* __restrict__ tab, int nk, const float
 
 }  // namespace
 
+void dis_slot_params_into(const float* T, int n_states, int di, SlotParams* out) {
+  const double sd = (di == 1) ? -1.0 : 1.0;
+  const double sdm = (di == 1) ? 1.0 : -1.0;
+  for (int s = 0; s < n_states; ++s) {
+    SlotParams& p = out[s];
+    for (int a = 0; a < 3; ++a) p.t[a] = sd * (double)T[a * n_states + s];
+    for (int m = 0; m < 3; ++m) {
+      double th = wrap_to_pi((double)T[(3 + m) * n_states + s]);
+      p.flip[m] = std::fabs(th) > M_PI / 2 ? 1 : 0;
+      th = wrap_to_pi_half(th);
+      const double t2 = std::tan(th / 2);
+      p.tau[m] = sdm * t2;
+      p.sig[m] = sd * std::sin(th);
+      p.g2[m] = (1 + t2 * t2) / 2;
+      p.g3[m] = std::cos(th);
+    }
+  }
+}
+
 void dis_slot_params(const float* T, int n_states, const int* slots, int n_slots, int di,
                      std::vector<SlotParams>* out) {
   out->resize(n_slots);
@@ -86,6 +105,65 @@ void dis_slot_params(const float* T, int n_states, const int* slots, int n_slots
       p.g3[m] = std::cos(th);
     }
   }
+}
+
+// Forward/inverse transform tables for ns <= kMaxStaticSlots slots placed in
+// the caller's region [base, base+cap) with no heap use on the host or the
+// device: the per-slot scalars are staged in a stack array. Returns OOM when
+// the tables do not fit in cap bytes. Flip-slot lists are not built (the
+// caller rejects rotations beyond 90 degrees).
+int dis_build_tables_into(disorder_ctx_s* ctx, const disorder_plan_s* plan, const SlotParams* sp, int ns,
+                          char* base, size_t cap, Tables* tb) {
+  if (ns < 1 || ns > kMaxStaticSlots) return dis_set_error(ctx, DISORDER_BAD_ARG, "tables: %d slots", ns);
+  Workspace ws;
+  ws.base = base;
+  ws.cap = cap;
+  ws.off = 0;
+  const int* N = plan->N;
+  double h[15 * kMaxStaticSlots];
+  for (int j = 0; j < ns; ++j)
+    for (int m = 0; m < 3; ++m) {
+      h[(0 * 3 + m) * ns + j] = sp[j].tau[m];
+      h[(1 * 3 + m) * ns + j] = sp[j].sig[m];
+      h[(2 * 3 + m) * ns + j] = sp[j].g2[m];
+      h[(3 * 3 + m) * ns + j] = sp[j].g3[m];
+      h[(4 * 3 + m) * ns + j] = sp[j].t[m];
+    }
+  double* d = ws.take<double>(15 * (size_t)ns);
+  if (!d) return DISORDER_OOM;
+  // a pageable-source copy is staged before the call returns
+  DIS_CUDA_TRY(cudaMemcpyAsync(d, h, 15 * (size_t)ns * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  tb->n_slots = ns;
+  const int blocks = 2 * ctx->sm_count;
+  for (int m = 0; m < 3; ++m) {
+    const int a1 = TR0[m], a2 = TR1[m];
+    tb->e2s[m] = (long long)N[a1] * N[a2];
+    tb->e3s[m] = (long long)N[a2] * N[a1];
+    tb->e2[m] = ws.take<float2>(tb->e2s[m] * ns);
+    tb->e3[m] = ws.take<float2>(tb->e3s[m] * ns);
+    tb->g2[m] = tb->g3[m] = nullptr;
+    if (!tb->e2[m] || !tb->e3[m]) return DISORDER_OOM;
+    shear_table_kernel<<<blocks, 256, 0, ctx->stream>>>(tb->e2[m], nullptr, N[a1], N[a2], plan->d_kG[a1],
+                                                        plan->d_rG[a2], d + (0 * 3 + m) * ns, d + (2 * 3 + m) * ns,
+                                                        +1, 1.0 / N[a1], ns);
+    shear_table_kernel<<<blocks, 256, 0, ctx->stream>>>(tb->e3[m], nullptr, N[a2], N[a1], plan->d_kG[a2],
+                                                        plan->d_rG[a1], d + (1 * 3 + m) * ns, d + (3 * 3 + m) * ns,
+                                                        -1, 1.0 / N[a2], ns);
+    dis_count(ctx, 2);
+  }
+  for (int a = 0; a < 3; ++a) {
+    tb->e1s[a] = N[a];
+    tb->e1[a] = ws.take<float2>((size_t)N[a] * ns);
+    if (!tb->e1[a]) return DISORDER_OOM;
+    trans_table_kernel<<<blocks, 256, 0, ctx->stream>>>(tb->e1[a], N[a], plan->d_kG[a], d + (4 * 3 + a) * ns, ns);
+    dis_count(ctx);
+  }
+  for (int m = 0; m < 3; ++m) {
+    tb->any_flip[m] = false;
+    tb->d_flip_slots[m] = nullptr;
+  }
+  DIS_CUDA_TRY(cudaGetLastError());
+  return DISORDER_OK;
 }
 
 int dis_build_tables(disorder_ctx_s* ctx, const disorder_plan_s* plan, const std::vector<SlotParams>& sp,

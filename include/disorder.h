@@ -102,6 +102,24 @@ int disorder_sinc_rigid_transform(disorder_ctx ctx, disorder_plan plan, const vo
                                   int32_t x_states, const float* T, int32_t n_states,
                                   int32_t di, int32_t sumR, int32_t useFull, void* out);
 
+/* The sinc rigid transform above for callers that cannot let a library
+ * allocate device memory (an application that reserves its whole device
+ * budget at start-up and serves buffers from its own allocator, where a
+ * cudaMalloc can fail and synchronises the device). No counterpart in the
+ * reference. It allocates nothing: its scratch (the phase tables) lives in
+ * one static 32 MiB device array that every GPU loading this library holds
+ * until exit. Limits: at most 256 states and at most 32 MiB of tables per call
+ * (about 12 states at 256x256x176, about 200 at 64x64x44), rotations within
+ * +-90 degrees, and di=0 (inverse) takes n_states volumes and writes them
+ * back without summing. Larger requests fail with DISORDER_BAD_ARG. The first
+ * call on a device resolves the array's device address (cudaGetSymbolAddress)
+ * and should come before any stream capture. All calls share the one array:
+ * calls that overlap on the GPU (other streams or threads) race with each
+ * other. The plan must already exist (disorder_plan_create allocates). */
+int disorder_sinc_rigid_transform_static(disorder_ctx ctx, disorder_plan plan, const void* x,
+                                         int32_t x_states, const float* T, int32_t n_states,
+                                         int32_t di, int32_t useFull, void* out);
+
 /* G=sincRigidTransformGradient(xB,et,etg,F,FH)
  * (Methods/sincRigidTransformGradient.m:1-150) for the forward transform of
  * one volume x (device) by n_states transforms T (host). G: device, 6 x
