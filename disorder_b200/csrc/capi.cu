@@ -231,6 +231,23 @@ int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* g, const di
     p->rG[m].assign(g->rG[m], g->rG[m] + g->N[m]);
     p->kG[m].assign(g->kG[m], g->kG[m] + g->N[m]);
     p->cent[m] = g->cent[m];
+    // kG linear in the signed frequency (DC first, as generateTransformGrids
+    // with sh=1 builds it): kG[k] ~ alpha * (k < N/2 ? k : k - N). The
+    // pipelined passes then generate their phase factors from per-row seeds.
+    const int n = p->N[m];
+    double sxy = 0, sxx = 0;
+    for (int k = 0; k < n; ++k) {
+      const double kv = (k < n / 2 + (n & 1)) ? k : k - n;
+      sxy += kv * p->kG[m][k];
+      sxx += kv * kv;
+    }
+    p->k_alpha[m] = sxx > 0 ? sxy / sxx : 0.0;
+    p->k_linear[m] = (n % 2 == 0) && sxx > 0;
+    for (int k = 0; k < n && p->k_linear[m]; ++k) {
+      const double kv = (k < n / 2) ? k : k - n;
+      const double want = p->k_alpha[m] * kv, got = p->kG[m][k];
+      if (std::fabs(got - want) > 4.0 * 1.2e-7 * std::fabs(want) + 1e-30) p->k_linear[m] = false;
+    }
   }
   p->V = (long long)p->N[0] * p->N[1] * p->N[2];
   for (int m = 0; m < 3; ++m) {

@@ -32,7 +32,9 @@ bool dis_any_motion(const float* T, int n) {
 size_t dis_table_bytes(const disorder_plan_s* plan, int ns, bool grad) {
   const long long N0 = plan->N[0], N1 = plan->N[1], N2 = plan->N[2];
   const long long shear = 2 * (N0 * N1 + N2 * N0 + N1 * N2);
-  return (size_t)ns * (sizeof(float2) * (shear * (grad ? 2 : 1) + N0 + N1 + N2) + 15 * sizeof(double)) + 64 * 1024;
+  const long long seeds = 34 * (3 * (N0 + N1 + N2) + 3);  // rows of at most 2*16+2 seeds
+  return (size_t)ns * (sizeof(float2) * (shear * (grad ? 2 : 1) + N0 + N1 + N2 + seeds) + 15 * sizeof(double)) +
+         64 * 1024;
 }
 
 static CoilArgs coil_args(const disorder_plan_s* plan, const float2* Sf, int C, int n3_lo, int N3c, long long Vz,

@@ -2,7 +2,20 @@
 // instantiated in fast_[a-e].cu (one translation unit per group of sizes).
 #include "fastpass.cuh"
 #include "fastpass.h"
+#include "pipepass.cuh"
 #include "plane.cuh"
+
+extern template struct fp::PipeLaunch<4, 4>;
+extern template struct fp::PipeLaunch<8, 4>;
+extern template struct fp::PipeLaunch<4, 11>;
+extern template struct fp::PipeLaunch<8, 8>;
+extern template struct fp::PipeLaunch<8, 11>;
+extern template struct fp::PipeLaunch<8, 12>;
+extern template struct fp::PipeLaunch<16, 8>;
+extern template struct fp::PipeLaunch<16, 10>;
+extern template struct fp::PipeLaunch<16, 11>;
+extern template struct fp::PipeLaunch<16, 12>;
+extern template struct fp::PipeLaunch<16, 16>;
 
 extern template struct fp::Launch<4, 4>;
 extern template struct fp::Launch<8, 4>;
@@ -41,6 +54,23 @@ bool dis_fast_factor(int n, int* F1, int* F2) {
     case 176: *F1 = 16; *F2 = 11; return true;
     case 192: *F1 = 16; *F2 = 12; return true;
     case 256: *F1 = 16; *F2 = 16; return true;
+    default: return false;
+  }
+}
+
+bool dis_fast_pipe(const LinePassArgs& a, const float2* tw, cudaStream_t s) {
+  switch (a.N[a.axis]) {
+    case 16: return fp::PipeLaunch<4, 4>::run(a, tw, s);
+    case 32: return fp::PipeLaunch<8, 4>::run(a, tw, s);
+    case 44: return fp::PipeLaunch<4, 11>::run(a, tw, s);
+    case 64: return fp::PipeLaunch<8, 8>::run(a, tw, s);
+    case 88: return fp::PipeLaunch<8, 11>::run(a, tw, s);
+    case 96: return fp::PipeLaunch<8, 12>::run(a, tw, s);
+    case 128: return fp::PipeLaunch<16, 8>::run(a, tw, s);
+    case 160: return fp::PipeLaunch<16, 10>::run(a, tw, s);
+    case 176: return fp::PipeLaunch<16, 11>::run(a, tw, s);
+    case 192: return fp::PipeLaunch<16, 12>::run(a, tw, s);
+    case 256: return fp::PipeLaunch<16, 16>::run(a, tw, s);
     default: return false;
   }
 }

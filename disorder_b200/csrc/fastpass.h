@@ -7,6 +7,9 @@ bool dis_fast_factor(int n, int* F1, int* F2);
 // Each returns false when n has no fast kernel (the caller then uses the
 // generic shared-memory Stockham kernels).
 bool dis_fast_line(const LinePassArgs& a, const float2* tw, cudaStream_t s);
+// Pipelined persistent kernel (pipepass.cuh) for the single-input passes;
+// false when the pass does not fit it.
+bool dis_fast_pipe(const LinePassArgs& a, const float2* tw, cudaStream_t s);
 bool dis_fast_expand(int n, const CoilArgs& a, const float2* z, float2* A, const float2* tw, cudaStream_t s);
 bool dis_fast_combine(int n, const CoilArgs& a, const float2* A, float2* u, float scale, const float2* tw,
                       cudaStream_t s);

@@ -68,10 +68,15 @@ struct disorder_plan_s {
   int* d_seg_of = nullptr;  // segment of each sample
   long long* d_seg_off = nullptr;
   float2* d_tw[3] = {nullptr, nullptr, nullptr};  // exp(-2 pi i m / N[axis]), m < N[axis]
+  // kG[axis][k] = k_alpha * (k < N/2 ? k : k - N) to within 4 ulp (even N)
+  double k_alpha[3] = {0, 0, 0};
+  bool k_linear[3] = {false, false, false};
 };
 
 // true unless DISORDER_GENERIC_FFT=1 forces the generic shared-memory kernels
 bool dis_use_fast();
+// true unless DISORDER_NO_PIPE=1 keeps every pass on the one-tile-per-CTA kernels
+bool dis_use_pipe();
 
 // ---------------------------------------------------------------- line pass
 enum { P_ZERO = 0, P_A = 1, P_B = 2, P_ONE = 3, P_DK = 4 };
@@ -100,6 +105,11 @@ struct LinePassArgs {
   long long out1_s;
   TabRef A, B, T;
   int c00, c01, c10, c11;
+  // Per-row phase seeds of the whole coefficient (c00 times T) for the
+  // pipelined kernel, [slot][row][sd_w] (tables.cu, seed_table_kernel);
+  // Sd.p == nullptr: use A and T.
+  TabRef Sd;
+  int sd_w;
   const float* kG;  // device kGrid along the axis (P_DK)
   const float2* tw;  // device twiddle table of the axis
   FFTPlan plan;
@@ -134,6 +144,16 @@ struct Tables {
   bool any_flip[3] = {false, false, false};
   std::vector<int> flip_slots[3];
   int* d_flip_slots[3] = {nullptr, nullptr, nullptr};
+  // Phase seeds (null when some axis has no pipelined kernel or a
+  // non-linear kGrid): sd2[m] / sd3[m] for the e2 / e3 passes of rotation m,
+  // sd2t for the last e2 pass with et{1}{2} fused, sd1[a] for the
+  // translation passes. Strides are elements per slot, widths per row.
+  float2* sd2[3] = {nullptr, nullptr, nullptr};
+  float2* sd3[3] = {nullptr, nullptr, nullptr};
+  float2* sd1[3] = {nullptr, nullptr, nullptr};
+  float2* sd2t = nullptr;
+  long long sd2s[3] = {0, 0, 0}, sd3s[3] = {0, 0, 0}, sd1s[3] = {0, 0, 0}, sd2ts = 0;
+  int sdw[3] = {0, 0, 0};  // row width of seeds along axis a (2*F1 + 2)
 };
 
 void dis_slot_params(const float* T, int n_states, const int* slots, int n_slots, int di,

@@ -23,6 +23,8 @@ LinePassArgs base_args(const disorder_plan_s* plan, int axis, int n_slots) {
   a.out0 = a.out1 = nullptr;
   a.in0_s = a.in1_s = a.out0_s = a.out1_s = 0;
   a.c00 = a.c01 = a.c10 = a.c11 = P_ZERO;
+  a.Sd = TabRef();
+  a.sd_w = 0;
   a.kG = plan->d_kG[axis];
   a.tw = plan->d_tw[axis];
   a.plan = plan->fft[axis];
@@ -45,12 +47,32 @@ LinePassArgs shear_args(const disorder_plan_s* plan, const Tables& tb, int m, in
   if (which == 0) {
     a.A = tab(tb.e2[m], tb.e2s[m], a2);
     a.B = tab(tb.g2[m], tb.e2s[m], a2);
+    a.Sd = tab(tb.sd2[m], tb.sd2s[m], a2);
+    a.sd_w = tb.sdw[a1];
   } else {
     a.A = tab(tb.e3[m], tb.e3s[m], a1);
     a.B = tab(tb.g3[m], tb.e3s[m], a1);
+    a.Sd = tab(tb.sd3[m], tb.sd3s[m], a1);
+    a.sd_w = tb.sdw[a2];
   }
   a.c00 = P_A;
   return a;
+}
+
+// The coefficient setters below keep the table form (A, T) and the seed
+// form (Sd) of a pass in step.
+// translation-only pass along ax: (1/N) et{1}{ax}
+void set_translation(LinePassArgs& a, const Tables& tb, int ax) {
+  a.c00 = P_ONE;
+  a.T = tab(tb.e1[ax], tb.e1s[ax], -1);
+  a.Sd = tab(tb.sd1[ax], tb.sd1s[ax], -1);
+  a.sd_w = tb.sdw[ax];
+}
+
+// et{1}{2} fused into the last e2 pass of rotation 3 (single-input form)
+void fuse_t1(LinePassArgs& a, const Tables& tb) {
+  a.T = tab(tb.e1[1], tb.e1s[1], -1);
+  a.Sd = tab(tb.sd2t, tb.sd2ts, TR1[2]);
 }
 
 void io(LinePassArgs& a, const float2* in, long long in_s, float2* out, long long out_s) {
@@ -117,17 +139,15 @@ int rotations_and_translation(disorder_ctx_s* ctx, const disorder_plan_s* plan, 
     DIS_TRY(dis_line_pass(ctx, a));
     a = shear_args(plan, tb, m, 0, ns);
     io(a, w, V, w, V);
-    if (m == 2) a.T = tab(tb.e1[1], tb.e1s[1], -1);
+    if (m == 2) fuse_t1(a, tb);
     DIS_TRY(dis_line_pass(ctx, a));
   }
   LinePassArgs a = base_args(plan, 0, ns);
-  a.c00 = P_ONE;
-  a.T = tab(tb.e1[0], tb.e1s[0], -1);
+  set_translation(a, tb, 0);
   io(a, w, V, w, V);
   DIS_TRY(dis_line_pass(ctx, a));
   a = base_args(plan, 2, ns);
-  a.c00 = P_ONE;
-  a.T = tab(tb.e1[2], tb.e1s[2], -1);
+  set_translation(a, tb, 2);
   io(a, w, V, out, V);
   DIS_TRY(dis_line_pass(ctx, a));
   return DISORDER_OK;
@@ -151,8 +171,7 @@ int dis_forward_transform(disorder_ctx_s* ctx, const disorder_plan_s* plan, cons
     // translations only: DFT along every axis, et{1}, inverse DFT (:59-64)
     for (int ax = 0; ax < 3; ++ax) {
       LinePassArgs a = base_args(plan, ax, ns);
-      a.c00 = P_ONE;
-      a.T = tab(tb.e1[ax], tb.e1s[ax], -1);
+      set_translation(a, tb, ax);
       io(a, cur, cur_s, z, V);
       DIS_TRY(dis_line_pass(ctx, a));
       cur = z;
@@ -186,20 +205,18 @@ int dis_forward_transform(disorder_ctx_s* ctx, const disorder_plan_s* plan, cons
     DIS_TRY(dis_line_pass(ctx, a));
     a = shear_args(plan, tb, m, 0, ns);
     io(a, z, V, z, V);
-    if (m == 2 && useFull != -1) a.T = tab(tb.e1[1], tb.e1s[1], -1);  // et{1}{2} fused (:57-72)
+    if (m == 2 && useFull != -1) fuse_t1(a, tb);  // et{1}{2} fused (:57-72)
     DIS_TRY(dis_line_pass(ctx, a));
     cur = z;
     cur_s = V;
   }
   if (useFull != -1) {
     LinePassArgs a = base_args(plan, 0, ns);
-    a.c00 = P_ONE;
-    a.T = tab(tb.e1[0], tb.e1s[0], -1);
+    set_translation(a, tb, 0);
     io(a, z, V, z, V);
     DIS_TRY(dis_line_pass(ctx, a));
     a = base_args(plan, 2, ns);
-    a.c00 = P_ONE;
-    a.T = tab(tb.e1[2], tb.e1s[2], -1);
+    set_translation(a, tb, 2);
     io(a, z, V, z, V);
     DIS_TRY(dis_line_pass(ctx, a));
   }
@@ -220,8 +237,7 @@ int dis_inverse_transform(disorder_ctx_s* ctx, const disorder_plan_s* plan, floa
   if (useFull == 0) {
     for (int ax = 0; ax < 3; ++ax) {
       LinePassArgs a = base_args(plan, ax, ns);
-      a.c00 = P_ONE;
-      a.T = tab(tb.e1[ax], tb.e1s[ax], -1);
+      set_translation(a, tb, ax);
       io(a, u, V, u, V);
       if (ax == 2 && out) {
         a.accumulate = 1;
@@ -235,8 +251,7 @@ int dis_inverse_transform(disorder_ctx_s* ctx, const disorder_plan_s* plan, floa
   if (useFull != -1) {
     for (int ax : {2, 0}) {
       LinePassArgs a = base_args(plan, ax, ns);
-      a.c00 = P_ONE;
-      a.T = tab(tb.e1[ax], tb.e1s[ax], -1);
+      set_translation(a, tb, ax);
       io(a, u, V, u, V);
       DIS_TRY(dis_line_pass(ctx, a));
     }
@@ -245,7 +260,7 @@ int dis_inverse_transform(disorder_ctx_s* ctx, const disorder_plan_s* plan, floa
   for (int m = 2; m >= 0; --m) {
     LinePassArgs a = shear_args(plan, tb, m, 0, ns);
     io(a, u, V, u, V);
-    if (m == 2 && useFull != -1) a.T = tab(tb.e1[1], tb.e1s[1], -1);
+    if (m == 2 && useFull != -1) fuse_t1(a, tb);
     DIS_TRY(dis_line_pass(ctx, a));
     a = shear_args(plan, tb, m, 1, ns);
     io(a, u, V, u, V);
@@ -355,13 +370,11 @@ int dis_gradient(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2*
       DIS_TRY(rotations_and_translation(ctx, plan, tb, m + 1, w1, g));
     } else {
       LinePassArgs t = base_args(plan, 0, ns);
-      t.c00 = P_ONE;
-      t.T = tab(tb.e1[0], tb.e1s[0], -1);
+      set_translation(t, tb, 0);
       io(t, w1, V, w1, V);
       DIS_TRY(dis_line_pass(ctx, t));
       t = base_args(plan, 2, ns);
-      t.c00 = P_ONE;
-      t.T = tab(tb.e1[2], tb.e1s[2], -1);
+      set_translation(t, tb, 2);
       io(t, w1, V, g, V);
       DIS_TRY(dis_line_pass(ctx, t));
     }

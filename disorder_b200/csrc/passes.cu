@@ -234,10 +234,25 @@ bool dis_use_fast() {
   return v == 1;
 }
 
+// DISORDER_NO_PIPE=1 keeps every pass on the one-tile-per-CTA kernels.
+bool dis_use_pipe() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = std::getenv("DISORDER_NO_PIPE");
+    v = (e && e[0] == '1') ? 0 : 1;
+  }
+  return v == 1;
+}
+
 int dis_line_pass(disorder_ctx_s* ctx, LinePassArgs a) {
   const int n = a.N[a.axis];
   if (a.plan.n != n) return dis_set_error(ctx, DISORDER_BAD_ARG, "line pass: plan size %d != axis size %d", a.plan.n, n);
   if (a.n_slots == 0) return DISORDER_OK;
+  if (dis_use_fast() && a.tw && dis_use_pipe() && dis_fast_pipe(a, a.tw, ctx->stream)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   if (dis_use_fast() && a.tw && dis_fast_line(a, a.tw, ctx->stream)) {
     dis_count(ctx);
     DIS_CUDA_TRY(cudaGetLastError());

@@ -6,6 +6,7 @@
 // DFT of the pass that applies a factor is folded into that factor.
 #include <cmath>
 
+#include "fastpass.h"
 #include "internal.h"
 
 namespace {
@@ -62,6 +63,84 @@ __global__ void trans_table_kernel(float2* __restrict__ tab, int nk, const float
     sincos(t[slot] * (double)kG[k], &s, &c);
     tab[e] = make_float2((float)c, (float)s);
   }
+}
+
+// Seeds of the coefficient invn * exp(i*phi*kG[k]) along a pass axis of
+// even length N = F1*F2 whose kGrid is linear, kG[k] = alpha*kv(k) with
+// kv(k) = k for k < N/2 and k - N beyond, for phi = coef[slot]*rG[row] +
+// t[slot] (either term may be absent). Row `row` of slot `slot` holds
+//   [j]        invn * exp(i*phi*alpha*j)                   j < F1
+//   [F1 + j]   invn * exp(i*phi*alpha*(j + F1*k2h - N))    j < F1, k2h = ceil(F2/2)
+//   [2*F1]     exp(i*phi*alpha*F1)                         (the step in k2)
+//   [2*F1+1]   0                                           (pads rows to 16 bytes)
+// so that the coefficient of frequency k = j + F1*k2 is lo[j]*step^k2 on the
+// non-negative side and hi[j]*step^(k2-k2h) on the negative side. The phase
+// is formed in double precision from rG*alpha*kv, where the e2/e3 tables
+// round the product rG*kG to single first (Methods/generateTransformGrids.m:57-62).
+__global__ void seed_table_kernel(float2* __restrict__ tab, int nr, int sw, int F1, int N, int k2h, double alpha,
+                                  double invn, const float* __restrict__ rG, const double* __restrict__ coef,
+                                  const double* __restrict__ t, int n_slots) {
+  const long long per = (long long)nr * sw;
+  const long long tot = per * n_slots;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+    const int slot = (int)(e / per);
+    const long long rem = e - slot * per;
+    const int r = (int)(rem / sw), j = (int)(rem - (long long)r * sw);
+    double phi = 0.0;
+    if (coef) phi += coef[slot] * (double)rG[r];
+    if (t) phi += t[slot];
+    double kv, sc = invn;
+    if (j < F1) {
+      kv = j;
+    } else if (j < 2 * F1) {
+      kv = (double)(j - F1) + (double)F1 * k2h - N;
+    } else if (j == 2 * F1) {
+      kv = F1;
+      sc = 1.0;
+    } else {
+      tab[e] = make_float2(0.f, 0.f);
+      continue;
+    }
+    double s, c;
+    sincos(phi * alpha * kv, &s, &c);
+    tab[e] = make_float2((float)(c * sc), (float)(s * sc));
+  }
+}
+
+// Seed tables of the pipelined passes (left null, and the passes on the
+// e1/e2/e3 tables, unless every axis has a pipelined kernel and a linear
+// kGrid). d: the per-slot scalars [what][m][slot] of dis_build_tables.
+int build_seeds(disorder_ctx_s* ctx, const disorder_plan_s* plan, const double* d, int ns, Workspace* ws,
+                Tables* tb) {
+  if (!dis_use_fast() || !dis_use_pipe()) return DISORDER_OK;
+  const int* N = plan->N;
+  int F1[3], F2[3];
+  for (int a = 0; a < 3; ++a)
+    if (!dis_fast_factor(N[a], &F1[a], &F2[a]) || !plan->k_linear[a]) return DISORDER_OK;
+  for (int a = 0; a < 3; ++a) tb->sdw[a] = 2 * F1[a] + 2;
+  const int blocks = 2 * ctx->sm_count;
+  auto make = [&](int ax, int nr, const float* rG, const double* coef, const double* t, long long* stride) -> float2* {
+    *stride = (long long)nr * tb->sdw[ax];
+    float2* p = ws->take<float2>((size_t)(*stride) * ns);
+    if (!p) return nullptr;
+    seed_table_kernel<<<blocks, 256, 0, ctx->stream>>>(p, nr, tb->sdw[ax], F1[ax], N[ax], (F2[ax] + 1) / 2,
+                                                       plan->k_alpha[ax], 1.0 / N[ax], rG, coef, t, ns);
+    dis_count(ctx);
+    return p;
+  };
+  for (int m = 0; m < 3; ++m) {
+    const int a1 = TR0[m], a2 = TR1[m];
+    tb->sd2[m] = make(a1, N[a2], plan->d_rG[a2], d + (0 * 3 + m) * ns, nullptr, &tb->sd2s[m]);
+    tb->sd3[m] = make(a2, N[a1], plan->d_rG[a1], d + (1 * 3 + m) * ns, nullptr, &tb->sd3s[m]);
+    if (!tb->sd2[m] || !tb->sd3[m]) return dis_set_error(ctx, DISORDER_OOM, "tables: workspace too small");
+  }
+  tb->sd2t = make(TR0[2], N[TR1[2]], plan->d_rG[TR1[2]], d + (0 * 3 + 2) * ns, d + (4 * 3 + 1) * ns, &tb->sd2ts);
+  if (!tb->sd2t) return dis_set_error(ctx, DISORDER_OOM, "tables: workspace too small");
+  for (int a = 0; a < 3; ++a) {
+    tb->sd1[a] = make(a, 1, nullptr, nullptr, d + (4 * 3 + a) * ns, &tb->sd1s[a]);
+    if (!tb->sd1[a]) return dis_set_error(ctx, DISORDER_OOM, "tables: workspace too small");
+  }
+  return DISORDER_OK;
 }
 
 }  // namespace
@@ -217,6 +296,7 @@ int dis_build_tables(disorder_ctx_s* ctx, const disorder_plan_s* plan, const std
     trans_table_kernel<<<blocks, 256, 0, ctx->stream>>>(tb->e1[a], N[a], plan->d_kG[a], d + (4 * 3 + a) * ns, ns);
     dis_count(ctx);
   }
+  DIS_TRY(build_seeds(ctx, plan, d, ns, ws, tb));
   for (int m = 0; m < 3; ++m) {
     tb->flip_slots[m].clear();
     for (int j = 0; j < ns; ++j)
