@@ -24,8 +24,8 @@ constexpr int pow2ceil(int x) {
   return p;
 }
 
-// exp(-2 pi i q / R) for the small DFTs comes from the N-point twiddle table
-// in shared memory: tw[q * (N / R)].
+// exp(-2 pi i q / R) for the small DFTs comes from an R-point twiddle table
+// in shared memory: tw[q * st] with st = 1 (see Tw below).
 
 // ---------------------------------------------------------------- small DFTs
 template <bool INV>
@@ -220,6 +220,41 @@ struct DFT<15, INV> : DFT2D<5, 3, INV> {};
 template <bool INV>
 struct DFT<9, INV> : DFT2D<3, 3, INV> {};
 
+// ---------------------------------------------------------------- twiddles
+// Shared-memory twiddles of a line FFT of length N = N1*N2 (SIZE float2):
+//   [k1*P + t]     W_N^{t k1}  (k1 < N1, t < N2): the four-step twiddles
+//   [W1 + q]       W_N1^q      (q < N1): the N1-point DFTs
+//   [W2 + q]       W_N2^q      (q < N2): the N2-point DFTs
+// The row pitch P is odd, so that the forward reads (fixed k1, consecutive t
+// across the lanes) and the inverse reads (fixed t, consecutive k1 across the
+// lanes, stride P) both hit 16 distinct 8-byte bank pairs.
+template <int N1, int N2>
+struct Tw {
+  static constexpr int P = (N2 % 2 == 0) ? N2 + 1 : N2 + 2;
+  static constexpr int W1 = N1 * P;
+  static constexpr int W2 = W1 + N1;
+  static constexpr int SIZE = (W2 + N2 + 1) & ~1;
+};
+
+// Fill the table above from the N-point table twg[m] = W_N^m (global memory).
+template <int N1, int N2>
+DIS_D void load_tw(float2* tws, const float2* __restrict__ twg, int tid, int nthr) {
+  using T = Tw<N1, N2>;
+  constexpr int N = N1 * N2;
+  for (int e = tid; e < T::SIZE; e += nthr) {
+    float2 v = make_float2(0.f, 0.f);
+    if (e < T::W1) {
+      const int k1 = e / T::P, t = e % T::P;
+      if (t < N2) v = twg[(t * k1) % N];
+    } else if (e < T::W2) {
+      v = twg[(e - T::W1) * N2];
+    } else if (e < T::W2 + N2) {
+      v = twg[(e - T::W2) * N1];
+    }
+    tws[e] = v;
+  }
+}
+
 // ---------------------------------------------------------------- line FFT
 template <int N1_, int N2_>
 struct Line {
@@ -227,15 +262,17 @@ struct Line {
   static constexpr int N2 = N2_;
   static constexpr int N = N1 * N2;
   static constexpr int TL = pow2ceil(Max<N1, N2>::v);  // threads per line
-  static constexpr int EX = N2 + 1;                    // exchange row pitch
+  static constexpr int EX = Tw<N1, N2>::P;             // exchange row pitch (odd: conflict-free)
   static constexpr int EXSZ = N1 * EX;                 // exchange tile per line (float2)
+  static constexpr int TWS = Tw<N1, N2>::SIZE;         // shared twiddle table (float2)
 
   // A -> B. a: layout A (used when t < N2); c: layout B (valid when t < N1)
   static DIS_D void fwd(float2 (&a)[N1], float2 (&c)[N2], int t, float2* ex, const float2* tw) {
+    using T = Tw<N1, N2>;
     if (t < N2) {
-      DFT<N1, false>::run(a, tw, N / N1);
+      DFT<N1, false>::run(a, tw + T::W1, 1);
 #pragma unroll
-      for (int k1 = 1; k1 < N1; ++k1) a[k1] = cmul(a[k1], tw[t * k1]);
+      for (int k1 = 1; k1 < N1; ++k1) a[k1] = cmul(a[k1], tw[k1 * T::P + t]);
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) ex[k1 * EX + t] = a[k1];
     }
@@ -243,17 +280,18 @@ struct Line {
     if (t < N1) {
 #pragma unroll
       for (int u = 0; u < N2; ++u) c[u] = ex[t * EX + u];
-      DFT<N2, false>::run(c, tw, N / N2);
+      DFT<N2, false>::run(c, tw + T::W2, 1);
     }
     __syncwarp();
   }
 
   // B -> A, unnormalised inverse.
   static DIS_D void inv(float2 (&c)[N2], float2 (&a)[N1], int t, float2* ex, const float2* tw) {
+    using T = Tw<N1, N2>;
     if (t < N1) {
-      DFT<N2, true>::run(c, tw, N / N2);
+      DFT<N2, true>::run(c, tw + T::W2, 1);
 #pragma unroll
-      for (int u = 1; u < N2; ++u) c[u] = cmulc(c[u], tw[u * t]);
+      for (int u = 1; u < N2; ++u) c[u] = cmulc(c[u], tw[t * T::P + u]);
 #pragma unroll
       for (int u = 0; u < N2; ++u) ex[t * EX + u] = c[u];
     }
@@ -261,7 +299,7 @@ struct Line {
     if (t < N2) {
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) a[k1] = ex[k1 * EX + t];
-      DFT<N1, true>::run(a, tw, N / N1);
+      DFT<N1, true>::run(a, tw + T::W1, 1);
     }
     __syncwarp();
   }

@@ -120,11 +120,11 @@ __global__ void __launch_bounds__(kThreads) line_kernel(LinePassArgs a, const fl
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* ex = sm + ((N + 1) & ~1);
+  float2* ex = sm + LN::TWS;
   float2* st = ex + LPB * LN::EXSZ;
   const int tid = threadIdx.x;
   const int lt = tid % TL, li = tid / TL;
-  for (int m = tid; m < N; m += kThreads) tw[m] = twg[m];
+  ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
   const LineInfo L = line_info(a.N, a.axis, LPB, blockIdx.x, li);
   const int rowA = a.A.b == 0 ? L.coord[0] : (a.A.b == 1 ? L.coord[1] : (a.A.b == 2 ? L.coord[2] : 0));
   const int rowB = a.B.b == 0 ? L.coord[0] : (a.B.b == 1 ? L.coord[1] : (a.B.b == 2 ? L.coord[2] : 0));
@@ -278,9 +278,9 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(CoilArgs a, const floa
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* ex = sm + ((N + 1) & ~1);
+  float2* ex = sm + LN::TWS;
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
-  for (int m = tid; m < N; m += kThreads) tw[m] = twg[m];
+  ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
   const long long nlines = (long long)a.N2 * a.N3c;
   const long long q = (long long)blockIdx.x * LPB + li;
   const bool valid = q < nlines && lt < F2;
@@ -316,9 +316,9 @@ __global__ void __launch_bounds__(kThreads) combine_kernel(CoilArgs a, const flo
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* ex = sm + ((N + 1) & ~1);
+  float2* ex = sm + LN::TWS;
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
-  for (int m = tid; m < N; m += kThreads) tw[m] = twg[m];
+  ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
   const long long nlines = (long long)a.N2 * a.N3c;
   const long long q = (long long)blockIdx.x * LPB + li;
   const bool ok = q < nlines;
@@ -379,10 +379,10 @@ __global__ void __launch_bounds__(kThreads) axis1_kernel(CoilArgs a, float2* __r
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL, P = LPB + 1;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* ex = sm + ((N + 1) & ~1);
+  float2* ex = sm + LN::TWS;
   float2* st = ex + LPB * LN::EXSZ;
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
-  for (int m = tid; m < N; m += kThreads) tw[m] = twg[m];
+  ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
   const int N1 = a.N1;
   const Tile1 t = tile1<LPB>(N1, blockIdx.x);
   const int c = blockIdx.y, slot = blockIdx.z;
@@ -465,7 +465,7 @@ struct Launch {
   using LN = ff::Line<F1, F2>;
   static constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
   static size_t smem(bool staged) {
-    return sizeof(float2) * (((N + 1) & ~1) + LPB * LN::EXSZ + (staged ? (size_t)N * (LPB + 1) : 0));
+    return sizeof(float2) * (LN::TWS + LPB * LN::EXSZ + (staged ? (size_t)N * (LPB + 1) : 0));
   }
   static bool init() {
     smem_attr(line_kernel<F1, F2, 0>);

@@ -42,10 +42,41 @@ struct Pipe {
   static constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL, TILE = N * LPB;
   static constexpr int EXT = LPB * LN::EXSZ;
   static constexpr int SB = ((TILE > EXT ? TILE : EXT) + 1) & ~1;  // one stage buffer, float2
-  static constexpr int TW = (N + 1) & ~1;                          // twiddles, float2
+  static constexpr int TW = LN::TWS;                               // twiddles, float2 (even)
   static constexpr size_t SMEM = sizeof(float2) * (TW + 2 * (size_t)SB);
+  // strided tiles move in 16-byte chunks: CPR per row, RS rows per sweep of the CTA
+  static constexpr int CPR = LPB / 2, RS = kThreads / CPR, SWEEPS = (N + RS - 1) / RS;
   static_assert(LPB >= 16, "the chunk swizzle needs at least 8 chunks per row");
+  static_assert(RS % 8 == 0, "a sweep must keep the row swizzle of each thread");
 };
+
+// One work item of a CTA: tile `tile` of slot `slot` and the tile's geometry
+// (32-bit: the volume holds fewer than 2^31 elements, checked on the host).
+//   axis 0:   lines q0 .. q0+nv-1 (q = n1 + N1*n2), base = q0*N0, (ca, cb) = (n1, n2) of line q0
+//   axis 1/2: lines n0 = ca .. ca+nv-1 at the other coordinate cb, base = first element
+struct PItem {
+  int tile, slot, base, nv, ca, cb;
+};
+
+DIS_D PItem pitem(const int* N, int axis, int lpb, int tile, int slot) {
+  PItem it;
+  it.tile = tile;
+  it.slot = slot;
+  if (axis == 0) {
+    const int q0 = tile * lpb;
+    it.nv = min(lpb, N[1] * N[2] - q0);
+    it.base = q0 * N[0];
+    it.cb = q0 / N[1];
+    it.ca = q0 - it.cb * N[1];
+  } else {
+    const int nt0 = (N[0] + lpb - 1) / lpb;
+    it.cb = tile / nt0;
+    it.ca = (tile - it.cb * nt0) * lpb;
+    it.nv = min(lpb, N[0] - it.ca);
+    it.base = axis == 1 ? it.ca + it.cb * N[0] * N[1] : it.ca + it.cb * N[0];
+  }
+  return it;
+}
 
 // ACC: out0 = beta*out0 + sum over the slots (each CTA owns whole tiles and
 // walks their slots in order); otherwise out0[slot] = pass(in0[slot]).
@@ -58,15 +89,14 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
                                                                      int n_tiles) {
   using P = Pipe<F1, F2>;
   using LN = typename P::LN;
-  constexpr int N = P::N, TL = P::TL, LPB = P::LPB, TILE = P::TILE, SB = P::SB;
+  constexpr int N = P::N, TL = P::TL, LPB = P::LPB, SB = P::SB, CPR = P::CPR, RS = P::RS;
   extern __shared__ __align__(16) float2 sm[];
   float2* tw = sm;
   float2* stg = sm + P::TW;
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
-  for (int m = tid; m < N; m += kThreads) tw[m] = twg[m];
+  ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
   const int axis = a.axis, S = a.n_slots, G = gridDim.x, b = blockIdx.x;
-  const long long sstr = axis_stride(a.N, axis);
-  const long long nlines0 = (long long)a.N[1] * a.N[2];
+  const int sstr = axis == 0 ? 1 : (axis == 1 ? a.N[0] : a.N[0] * a.N[1]);
   // n_tiles * S < 2^31 (checked on the host)
   int n_items;
   if (ACC)
@@ -75,83 +105,110 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
     const int nw = n_tiles * S;
     n_items = b < nw ? (nw - 1 - b) / G + 1 : 0;
   }
-  // item j of this CTA -> (tile, slot); without ACC the items are tile-major
-  // over the grid so that a shared input (in0_s == 0) is re-read from L2
-  auto item = [&](int j, int& tile, int& slot) {
+  if (n_items == 0) return;
+  // Item j of this CTA: with ACC, tile b + (j / S)*G and slot j % S; without,
+  // w = b + j*G, tile w / S and slot w % S (tile-major over the grid, so a
+  // shared input, in0_s == 0, is re-read from L2). Advanced incrementally.
+  const int gq = ACC ? 0 : G / S, gr = ACC ? 0 : G % S;
+  auto advance = [&](const PItem& c) {
+    int tile = c.tile, slot = c.slot;
     if (ACC) {
-      tile = b + (j / S) * G;
-      slot = j % S;
-    } else {
-      const int w = b + j * G;
-      tile = w / S;
-      slot = w % S;
-    }
-  };
-  auto issue = [&](int j, float2* st) {
-    int tile, slot;
-    item(j, tile, slot);
-    const float2* src = a.in0 + slot * a.in0_s;
-    if (axis == 0) {
-      const long long q0 = (long long)tile * LPB;
-      const int nl = (int)min((long long)LPB, nlines0 - q0);
-      const float2* g = src + q0 * N;
-      const int chunks = nl * (N / 2);
-#pragma unroll 1
-      for (int c = tid; c < chunks; c += kThreads) cp_async16(st + 2 * c, g + 2 * c);
-    } else {
-      long long base0;
-      int nv;
-      strided_tile(a.N, axis, LPB, tile, &base0, &nv);
-      const int cpr = nv >> 1;  // nv is even: N0 is even and tiles start at multiples of LPB
-      constexpr int CH = N * (LPB / 2);
-#pragma unroll 1
-      for (int c = tid; c < CH; c += kThreads) {
-        const int p = c / (LPB / 2), k = c % (LPB / 2);
-        if (k < cpr) cp_async16(st + swz<LPB>(p, 2 * k), src + base0 + 2 * k + p * sstr);
+      if (++slot == S) {
+        slot = 0;
+        tile += G;
       }
+    } else {
+      slot += gr;
+      tile += gq;
+      if (slot >= S) {
+        slot -= S;
+        ++tile;
+      }
+    }
+    return pitem(a.N, axis, LPB, tile, slot);
+  };
+  // per-thread constants of the strided chunk walk
+  const int ck = tid % CPR, cp0 = tid / CPR;
+  const int cso = swz<LPB>(cp0, 2 * ck);
+  auto issue = [&](const PItem& it, float2* st) {
+    const float2* src = a.in0 + it.slot * a.in0_s + it.base;
+    if (axis == 0) {
+      constexpr int CH = LPB * N / 2, IT = (CH + kThreads - 1) / kThreads;
+      if (it.nv == LPB) {
+#pragma unroll
+        for (int i = 0; i < IT; ++i) {
+          const int c = tid + i * kThreads;
+          if (CH % kThreads == 0 || c < CH) cp_async16(st + 2 * c, src + 2 * c);
+        }
+      } else {
+        const int chunks = it.nv * (N / 2);
+#pragma unroll 1
+        for (int c = tid; c < chunks; c += kThreads) cp_async16(st + 2 * c, src + 2 * c);
+      }
+    } else if (2 * ck < it.nv) {  // nv is even: N0 is even and tiles start at multiples of LPB
+      const float2* g = src + 2 * ck + cp0 * sstr;
+#pragma unroll
+      for (int i = 0; i < P::SWEEPS; ++i)
+        if (N % RS == 0 || cp0 + RS * i < N) cp_async16(st + cso + RS * i * LPB, g + (long long)RS * i * sstr);
     }
   };
 
   float2 acc[F1];
 #pragma unroll
   for (int m = 0; m < F1; ++m) acc[m] = make_float2(0.f, 0.f);
-  if (n_items > 0) issue(0, stg);
+  PItem cur = pitem(a.N, axis, LPB, ACC ? b : b / S, ACC ? 0 : b % S);
+  issue(cur, stg);
   cp_async_commit();
   for (int j = 0; j < n_items; ++j) {
     float2* st = stg + (j & 1) * SB;
-    if (j + 1 < n_items) issue(j + 1, stg + ((j + 1) & 1) * SB);
+    PItem nxt = cur;
+    if (j + 1 < n_items) {
+      nxt = advance(cur);
+      issue(nxt, stg + ((j + 1) & 1) * SB);
+    }
     cp_async_commit();
-    int tile, slot;
-    item(j, tile, slot);
-    const LineInfo L = line_info(a.N, axis, LPB, tile, li);
+    // this thread's line of the current item
+    const bool valid = li < cur.nv;
+    int c0 = 0, c1 = 0, c2 = 0;
+    if (axis == 0) {
+      c1 = cur.ca + li;
+      c2 = cur.cb;
+      while (c1 >= a.N[1]) {
+        c1 -= a.N[1];
+        ++c2;
+      }
+    } else {
+      c0 = cur.ca + li;
+      if (axis == 1)
+        c2 = cur.cb;
+      else
+        c1 = cur.cb;
+    }
     // phase seeds of this line, loaded while the tile lands
     float2 slo, shi, sst;
     if (SEED && lt < F1) {
-      const int row = a.Sd.b == 0 ? L.coord[0] : (a.Sd.b == 1 ? L.coord[1] : (a.Sd.b == 2 ? L.coord[2] : 0));
-      const float2* sr = a.Sd.p + slot * a.Sd.sstride + row * a.sd_w;
+      const int row = a.Sd.b == 0 ? c0 : (a.Sd.b == 1 ? c1 : (a.Sd.b == 2 ? c2 : 0));
+      const float2* sr = a.Sd.p + cur.slot * a.Sd.sstride + (valid ? row : 0) * a.sd_w;
       slo = sr[lt];
       shi = sr[F1 + lt];
       sst = sr[2 * F1];
     }
     cp_async_wait_1();
     __syncthreads();  // item j staged; twiddles visible
-    long long base0 = 0;
-    int nv = 0;
-    if (axis != 0) strided_tile(a.N, axis, LPB, tile, &base0, &nv);
     float2 v[F1], X[F2];
 #pragma unroll
     for (int m = 0; m < F1; ++m) {
       const int p = lt + F2 * m;
       float2 e = make_float2(0.f, 0.f);
-      if (lt < F2 && L.valid) e = axis == 0 ? st[li * N + p] : st[swz<LPB>(p, li)];
+      if (lt < F2 && valid) e = axis == 0 ? st[li * N + p] : st[swz<LPB>(p, li)];
       v[m] = e;
     }
     __syncthreads();  // the stage buffer becomes the exchange area
     float2* myex = st + li * LN::EXSZ;
     LN::fwd(v, X, lt, myex, tw);
     if (SEED && lt < F1) {
-      constexpr int KP = F2 / 2;             // k2 < KP: k < N/2 for every lt
-      constexpr bool ODD = (F2 & 1) != 0;    // odd F2: k2 == KP straddles N/2 at lt = F1/2
+      constexpr int KP = F2 / 2;           // k2 < KP: k < N/2 for every lt
+      constexpr bool ODD = (F2 & 1) != 0;  // odd F2: k2 == KP straddles N/2 at lt = F1/2
 #pragma unroll
       for (int k2 = 0; k2 < F2; ++k2) {
         float2 c;
@@ -167,9 +224,9 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
         X[k2] = cmul(c, X[k2]);
       }
     } else if (!SEED && lt < F1) {
-      const int rowA = a.A.b == 0 ? L.coord[0] : (a.A.b == 1 ? L.coord[1] : (a.A.b == 2 ? L.coord[2] : 0));
-      const float2* tA = a.A.p ? a.A.p + slot * a.A.sstride + (long long)rowA * N : nullptr;
-      const float2* tT = a.T.p ? a.T.p + slot * a.T.sstride : nullptr;
+      const int rowA = a.A.b == 0 ? c0 : (a.A.b == 1 ? c1 : (a.A.b == 2 ? c2 : 0));
+      const float2* tA = a.A.p ? a.A.p + cur.slot * a.A.sstride + (long long)(valid ? rowA : 0) * N : nullptr;
+      const float2* tT = a.T.p ? a.T.p + cur.slot * a.T.sstride : nullptr;
 #pragma unroll
       for (int k2 = 0; k2 < F2; ++k2) {
         const int k = lt + F1 * k2;
@@ -179,64 +236,59 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
       }
     }
     LN::inv(X, v, lt, myex, tw);
+    const bool last = !ACC || cur.slot == S - 1;
     if (ACC) {
 #pragma unroll
       for (int m = 0; m < F1; ++m) acc[m] = cadd(acc[m], v[m]);
-      if (slot == S - 1) {
-        const float beta = a.beta;
-        if (axis == 0) {
-          if (L.valid && lt < F2) {
+      if (last) {
 #pragma unroll
-            for (int m = 0; m < F1; ++m) {
-              const long long g = L.base + lt + F2 * m;
-              float2 o = acc[m];
-              if (beta != 0.f) o = cadd(o, cscale(a.out0[g], beta));
-              a.out0[g] = o;
-            }
-          }
-        } else {
-          __syncthreads();  // every line's exchange is done
-          if (lt < F2 && L.valid) {
-#pragma unroll
-            for (int m = 0; m < F1; ++m) st[swz<LPB>(lt + F2 * m, li)] = acc[m];
-          }
-          __syncthreads();
-          for (int e = tid; e < TILE; e += kThreads) {
-            const int p = e / LPB, l = e % LPB;
-            if (l < nv) {
-              const long long g = base0 + l + p * sstr;
-              float2 o = st[swz<LPB>(p, l)];
-              if (beta != 0.f) o = cadd(o, cscale(a.out0[g], beta));
-              a.out0[g] = o;
-            }
-          }
-        }
+        for (int m = 0; m < F1; ++m) v[m] = acc[m];
 #pragma unroll
         for (int m = 0; m < F1; ++m) acc[m] = make_float2(0.f, 0.f);
       }
-    } else if (axis == 0) {
-      float2* o0 = a.out0 + slot * a.out0_s;
-      if (L.valid && lt < F2) {
+    }
+    if (last) {
+      float2* o0 = a.out0 + (ACC ? 0 : cur.slot * a.out0_s) + cur.base;
+      const float beta = ACC ? a.beta : 0.f;
+      if (axis == 0) {
+        if (valid && lt < F2) {
+          float2* ol = o0 + li * N + lt;
 #pragma unroll
-        for (int m = 0; m < F1; ++m) o0[L.base + lt + F2 * m] = v[m];
-      }
-    } else {
-      __syncthreads();  // every line's exchange is done
-      if (lt < F2 && L.valid) {
+          for (int m = 0; m < F1; ++m) {
+            float2 o = v[m];
+            if (ACC && beta != 0.f) o = cadd(o, cscale(ol[F2 * m], beta));
+            ol[F2 * m] = o;
+          }
+        }
+      } else {
+        __syncthreads();  // every line's exchange is done
+        if (lt < F2 && valid) {
 #pragma unroll
-        for (int m = 0; m < F1; ++m) st[swz<LPB>(lt + F2 * m, li)] = v[m];
-      }
-      __syncthreads();
-      float2* o0 = a.out0 + slot * a.out0_s;
-      constexpr int IT = (TILE + kThreads - 1) / kThreads;
-#pragma unroll 4
-      for (int it = 0; it < IT; ++it) {
-        const int e = tid + it * kThreads;
-        const int p = e / LPB, l = e % LPB;
-        if (e < TILE && l < nv) o0[base0 + l + p * sstr] = st[swz<LPB>(p, l)];
+          for (int m = 0; m < F1; ++m) st[swz<LPB>(lt + F2 * m, li)] = v[m];
+        }
+        __syncthreads();
+        if (2 * ck < cur.nv) {
+          float2* g = o0 + 2 * ck + cp0 * sstr;
+#pragma unroll
+          for (int i = 0; i < P::SWEEPS; ++i) {
+            if (N % RS == 0 || cp0 + RS * i < N) {
+              float4 o = *reinterpret_cast<const float4*>(st + cso + RS * i * LPB);
+              float4* gp = reinterpret_cast<float4*>(g + (long long)RS * i * sstr);
+              if (ACC && beta != 0.f) {
+                const float4 q = *gp;
+                o.x += beta * q.x;
+                o.y += beta * q.y;
+                o.z += beta * q.z;
+                o.w += beta * q.w;
+              }
+              *gp = o;
+            }
+          }
+        }
       }
     }
     __syncthreads();  // the buffer is free for the copy issued by the next item
+    cur = nxt;
   }
   cp_async_wait_0();
 }
@@ -265,11 +317,14 @@ struct PipeLaunch {
     cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev);
     return o;
   }
-  // Whether the pass fits this kernel: one input, one output, coefficient
-  // A (or a constant) times the optional T row, 16-byte aligned slots, even N0.
+  // Whether the pass fits this kernel: one input, one output, coefficient A
+  // (or a constant) times the optional T row, 16-byte aligned volumes, even
+  // N0 and fewer than 2^31 elements per volume.
   static bool eligible(const LinePassArgs& a) {
     if (a.in1 || a.out1 || a.c01 != P_ZERO || a.c00 == P_B) return false;
-    if ((a.N[0] & 1) || (reinterpret_cast<uintptr_t>(a.in0) & 15) || (a.in0_s & 1)) return false;
+    if ((a.N[0] & 1) || (long long)a.N[0] * a.N[1] * a.N[2] >= (1LL << 31)) return false;
+    if ((reinterpret_cast<uintptr_t>(a.in0) & 15) || (a.in0_s & 1)) return false;
+    if ((reinterpret_cast<uintptr_t>(a.out0) & 15) || (a.out0_s & 1)) return false;
     return true;
   }
   static bool run(const LinePassArgs& a, const float2* tw, cudaStream_t s) {

@@ -55,7 +55,7 @@ struct Layout {
   using LN = ff::Line<F1, F2>;
   static constexpr int N1 = LN::N, TL = LN::TL, LPB = kThreads / TL, CB = LPB, XP = CB + 1;
   static size_t bytes(int N2, int C, int max_ns) {
-    const size_t f2 = ((N1 + 1) & ~1) + ((N2 + 1) & ~1) + (size_t)LPB * LN::EXSZ + (size_t)N1 * XP +
+    const size_t f2 = LN::TWS + ((N2 + 1) & ~1) + (size_t)LPB * LN::EXSZ + (size_t)N1 * XP +
                       (size_t)C * max_ns;
     const size_t ints = (size_t)N1 + 1 + 3 * (size_t)max_ns;
     return f2 * sizeof(float2) + ints * sizeof(int) + 64;
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kThreads) plane_kernel(PlaneArgs a, const floa
   extern __shared__ float2 sm[];
   const int N2 = a.N2;
   float2* tw1 = sm;
-  float2* tw2 = tw1 + ((N1 + 1) & ~1);
+  float2* tw2 = tw1 + LN::TWS;
   float2* ex = tw2 + ((N2 + 1) & ~1);
   float2* Xb = ex + LY::LPB * LN::EXSZ;
   float2* yv = Xb + N1 * XP;
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(kThreads) plane_kernel(PlaneArgs a, const floa
   const int seg = a.slot_seg[slot];
   const long long i0 = a.seg_off[seg];
   const int ns = (int)(a.seg_off[seg + 1] - i0);
-  for (int m = tid; m < N1; m += kThreads) tw1[m] = tw1g[m];
+  ff::load_tw<F1, F2>(tw1, tw1g, tid, kThreads);
   for (int m = tid; m < N2; m += kThreads) tw2[m] = tw2g[m];
   for (int q = tid; q < ns; q += kThreads) {
     s_ky[q] = a.ky[i0 + q];
