@@ -24,8 +24,47 @@ constexpr int pow2ceil(int x) {
   return p;
 }
 
-// exp(-2 pi i q / R) for the small DFTs comes from an R-point twiddle table
-// in shared memory: tw[q * st] with st = 1 (see Tw below).
+// ---------------------------------------------------------------- roots of unity
+// exp(-2 pi i q / R) for the small DFTs, evaluated at compile time from the
+// Taylor series of sin and cos about 0 (|angle| <= pi, 30 terms: converged
+// to double precision) and rounded to single; the kernels read them from
+// constant memory with compile-time offsets.
+constexpr double kPi = 3.14159265358979323846;
+constexpr double taylor_sin(double x) {
+  double t = x, s = x;
+  for (int n = 1; n < 30; ++n) {
+    t *= -x * x / ((2.0 * n) * (2.0 * n + 1));
+    s += t;
+  }
+  return s;
+}
+constexpr double taylor_cos(double x) {
+  double t = 1, s = 1;
+  for (int n = 1; n < 30; ++n) {
+    t *= -x * x / ((2.0 * n - 1) * (2.0 * n));
+    s += t;
+  }
+  return s;
+}
+template <int R>
+struct Roots {
+  float c[R];  // cos(2 pi q / R)
+  float s[R];  // -sin(2 pi q / R)
+  constexpr Roots() : c(), s() {
+    for (int q = 0; q < R; ++q) {
+      const double ang = 2 * kPi * (2 * q > R ? q - R : q) / R;
+      c[q] = (float)taylor_cos(ang);
+      s[q] = (float)(-taylor_sin(ang));
+    }
+  }
+};
+template <int R>
+__constant__ Roots<R> c_roots = Roots<R>();
+
+template <int R>
+DIS_D float2 root(int q) {  // W_R^q, q < R known at compile time after unrolling
+  return make_float2(c_roots<R>.c[q], c_roots<R>.s[q]);
+}
 
 // ---------------------------------------------------------------- small DFTs
 template <bool INV>
@@ -54,7 +93,7 @@ struct DFT {
         float2 A = v[0], B = make_float2(0.f, 0.f);
 #pragma unroll
         for (int r = 1; r <= H; ++r) {
-          const float2 w = tw[((q * r) % R) * st];  // (cos, -sin)
+          const float2 w = root<R>((q * r) % R);  // (cos, -sin)
           A.x = fmaf(a[r - 1].x, w.x, A.x);
           A.y = fmaf(a[r - 1].y, w.x, A.y);
           B.x = fmaf(b[r - 1].x, w.y, B.x);
@@ -71,7 +110,7 @@ struct DFT {
         float2 acc = v[0];
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          float2 w = tw[((q * r) % R) * st];
+          float2 w = root<R>((q * r) % R);
           if (INV) w.y = -w.y;
           acc = cfma(v[r], w, acc);
         }
@@ -173,7 +212,7 @@ struct DFT<16, INV> {
 
 // R = P*Q in registers (same four-step split as the line FFT):
 // X[k1 + P k2] = sum_j W_R^{j k1} W_Q^{j k2} sum_m W_P^{m k1} x[j + Q m].
-// tw[q*st] = W_R^q, so W_P^q = tw[q*Q*st] and W_Q^q = tw[q*P*st].
+// W_R^{j k1} comes from root<R>(); the P- and Q-point DFTs use their own roots.
 template <int P, int Q, bool INV>
 struct DFT2D {
   static DIS_D void run(float2* v, const float2* tw, int st) {
@@ -189,7 +228,7 @@ struct DFT2D {
         if (j == 0 || k1 == 0) {
           y[j][k1] = t[k1];
         } else {
-          float2 w = tw[((j * k1) % (P * Q)) * st];
+          float2 w = root<P * Q>((j * k1) % (P * Q));
           if (INV) w.y = -w.y;
           y[j][k1] = cmul(t[k1], w);
         }
