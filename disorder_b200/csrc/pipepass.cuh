@@ -23,31 +23,35 @@ DIS_D void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+DIS_D void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 DIS_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 DIS_D void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 DIS_D void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Element (p, l) of a strided-tile stage buffer: rows p of LPB elements, the
-// 16-byte chunks (element pairs) of row p XOR-permuted by p mod 8, so that
-// the reads of layout A (16 rows, 2 adjacent columns per warp) and the
-// row-wise copies both take the minimum number of shared-memory wavefronts.
-template <int LPB>
-DIS_D int swz(int p, int l) {
-  return p * LPB + (((((l >> 1) ^ (p & 7)) & (LPB / 2 - 1)) << 1) | (l & 1));
-}
-
+// Stage buffers are line-major: line l of the tile occupies
+// [l*pitch, l*pitch + N), and the same span (EXSZ <= pitch) is that line's
+// FFT exchange area once its data sit in registers, so a line's lanes only
+// synchronise among themselves (__syncwarp) between the two uses.
+//   axis 0:   pitch PL (even): each line is copied as 16-byte chunks;
+//   axis 1/2: pitch PS (odd): a tile row (one element of each line) is
+//             copied as 8-byte elements, and both the copies (consecutive
+//             lines, stride PS) and the FFT reads (consecutive elements of
+//             one line) hit distinct bank pairs.
 template <int F1, int F2>
 struct Pipe {
   using LN = ff::Line<F1, F2>;
-  static constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL, TILE = N * LPB;
-  static constexpr int EXT = LPB * LN::EXSZ;
-  static constexpr int SB = ((TILE > EXT ? TILE : EXT) + 1) & ~1;  // one stage buffer, float2
+  static constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
+  static constexpr int LEN = N > LN::EXSZ ? N : LN::EXSZ;
+  static constexpr int PL = (LEN + 1) & ~1, PS = LEN | 1;
+  static constexpr int SB = (LPB * (PL > PS ? PL : PS) + 1) & ~1;  // one stage buffer, float2
   static constexpr int TW = LN::TWS;                               // twiddles, float2 (even)
   static constexpr size_t SMEM = sizeof(float2) * (TW + 2 * (size_t)SB);
-  // strided tiles move in 16-byte chunks: CPR per row, RS rows per sweep of the CTA
-  static constexpr int CPR = LPB / 2, RS = kThreads / CPR, SWEEPS = (N + RS - 1) / RS;
-  static_assert(LPB >= 16, "the chunk swizzle needs at least 8 chunks per row");
-  static_assert(RS % 8 == 0, "a sweep must keep the row swizzle of each thread");
+  // strided copies: RS rows of the tile per sweep of the CTA
+  static constexpr int RS = kThreads / LPB, SWEEPS = (N + RS - 1) / RS;
+  static_assert(kThreads % LPB == 0, "whole rows per sweep");
 };
 
 // One work item of a CTA: tile `tile` of slot `slot` and the tile's geometry
@@ -89,7 +93,7 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
                                                                      int n_tiles) {
   using P = Pipe<F1, F2>;
   using LN = typename P::LN;
-  constexpr int N = P::N, TL = P::TL, LPB = P::LPB, SB = P::SB, CPR = P::CPR, RS = P::RS;
+  constexpr int N = P::N, TL = P::TL, LPB = P::LPB, SB = P::SB, PL = P::PL, PS = P::PS, RS = P::RS;
   extern __shared__ __align__(16) float2 sm[];
   float2* tw = sm;
   float2* stg = sm + P::TW;
@@ -127,29 +131,33 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
     }
     return pitem(a.N, axis, LPB, tile, slot);
   };
-  // per-thread constants of the strided chunk walk
-  const int ck = tid % CPR, cp0 = tid / CPR;
-  const int cso = swz<LPB>(cp0, 2 * ck);
+  // strided copies: this thread moves line sl, rows sp0 + RS*i
+  const int sl = tid % LPB, sp0 = tid / LPB;
   auto issue = [&](const PItem& it, float2* st) {
     const float2* src = a.in0 + it.slot * a.in0_s + it.base;
     if (axis == 0) {
-      constexpr int CH = LPB * N / 2, IT = (CH + kThreads - 1) / kThreads;
+      constexpr int CPL = N / 2, CH = LPB * CPL, IT = (CH + kThreads - 1) / kThreads;
       if (it.nv == LPB) {
 #pragma unroll
         for (int i = 0; i < IT; ++i) {
           const int c = tid + i * kThreads;
-          if (CH % kThreads == 0 || c < CH) cp_async16(st + 2 * c, src + 2 * c);
+          const int l = c / CPL, o = c - l * CPL;
+          if (CH % kThreads == 0 || c < CH) cp_async16(st + l * PL + 2 * o, src + 2 * c);
         }
       } else {
-        const int chunks = it.nv * (N / 2);
+        const int chunks = it.nv * CPL;
 #pragma unroll 1
-        for (int c = tid; c < chunks; c += kThreads) cp_async16(st + 2 * c, src + 2 * c);
+        for (int c = tid; c < chunks; c += kThreads) {
+          const int l = c / CPL, o = c - l * CPL;
+          cp_async16(st + l * PL + 2 * o, src + 2 * c);
+        }
       }
-    } else if (2 * ck < it.nv) {  // nv is even: N0 is even and tiles start at multiples of LPB
-      const float2* g = src + 2 * ck + cp0 * sstr;
+    } else if (sl < it.nv) {
+      const float2* g = src + sl + sp0 * sstr;
+      float2* d = st + sl * PS + sp0;
 #pragma unroll
       for (int i = 0; i < P::SWEEPS; ++i)
-        if (N % RS == 0 || cp0 + RS * i < N) cp_async16(st + cso + RS * i * LPB, g + (long long)RS * i * sstr);
+        if (N % RS == 0 || sp0 + RS * i < N) cp_async8(d + RS * i, g + (long long)RS * i * sstr);
     }
   };
 
@@ -161,12 +169,6 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
   cp_async_commit();
   for (int j = 0; j < n_items; ++j) {
     float2* st = stg + (j & 1) * SB;
-    PItem nxt = cur;
-    if (j + 1 < n_items) {
-      nxt = advance(cur);
-      issue(nxt, stg + ((j + 1) & 1) * SB);
-    }
-    cp_async_commit();
     // this thread's line of the current item
     const bool valid = li < cur.nv;
     int c0 = 0, c1 = 0, c2 = 0;
@@ -193,19 +195,22 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
       shi = sr[F1 + lt];
       sst = sr[2 * F1];
     }
-    cp_async_wait_1();
-    __syncthreads();  // item j staged; twiddles visible
+    cp_async_wait_0();
+    // item j staged (and twiddles visible); every thread is past item j-1,
+    // so the other buffer is free for the next item's copy
+    __syncthreads();
+    PItem nxt = cur;
+    if (j + 1 < n_items) {
+      nxt = advance(cur);
+      issue(nxt, stg + ((j + 1) & 1) * SB);
+    }
+    cp_async_commit();
+    float2* my = st + li * (axis == 0 ? PL : PS);
     float2 v[F1], X[F2];
 #pragma unroll
-    for (int m = 0; m < F1; ++m) {
-      const int p = lt + F2 * m;
-      float2 e = make_float2(0.f, 0.f);
-      if (lt < F2 && valid) e = axis == 0 ? st[li * N + p] : st[swz<LPB>(p, li)];
-      v[m] = e;
-    }
-    __syncthreads();  // the stage buffer becomes the exchange area
-    float2* myex = st + li * LN::EXSZ;
-    LN::fwd(v, X, lt, myex, tw);
+    for (int m = 0; m < F1; ++m) v[m] = (lt < F2 && valid) ? my[lt + F2 * m] : make_float2(0.f, 0.f);
+    __syncwarp();  // the line's span becomes its exchange area
+    LN::fwd(v, X, lt, my, tw);
     if (SEED && lt < F1) {
       constexpr int KP = F2 / 2;           // k2 < KP: k < N/2 for every lt
       constexpr bool ODD = (F2 & 1) != 0;  // odd F2: k2 == KP straddles N/2 at lt = F1/2
@@ -235,7 +240,7 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
         X[k2] = cmul(c, X[k2]);
       }
     }
-    LN::inv(X, v, lt, myex, tw);
+    LN::inv(X, v, lt, my, tw);
     const bool last = !ACC || cur.slot == S - 1;
     if (ACC) {
 #pragma unroll
@@ -251,6 +256,7 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
       float2* o0 = a.out0 + (ACC ? 0 : cur.slot * a.out0_s) + cur.base;
       const float beta = ACC ? a.beta : 0.f;
       if (axis == 0) {
+        // element lt + F2*m of this line, straight from registers
         if (valid && lt < F2) {
           float2* ol = o0 + li * N + lt;
 #pragma unroll
@@ -261,25 +267,29 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
           }
         }
       } else {
-        __syncthreads();  // every line's exchange is done
-        if (lt < F2 && valid) {
+        // back into the line's span, then tile rows as 16-byte pairs of lines
+        if (lt < F2) {
 #pragma unroll
-          for (int m = 0; m < F1; ++m) st[swz<LPB>(lt + F2 * m, li)] = v[m];
+          for (int m = 0; m < F1; ++m) my[lt + F2 * m] = v[m];
         }
         __syncthreads();
-        if (2 * ck < cur.nv) {
-          float2* g = o0 + 2 * ck + cp0 * sstr;
+        constexpr int PPR = LPB / 2, RO = kThreads / PPR;  // line pairs per row, rows per sweep
+        const int q = tid % PPR, r0 = tid / PPR;
+        if (2 * q < cur.nv) {  // nv is even: N0 is even and tiles start at multiples of LPB
+          const float2* s0 = st + 2 * q * PS + r0;
+          float2* g = o0 + 2 * q + (long long)r0 * sstr;
 #pragma unroll
-          for (int i = 0; i < P::SWEEPS; ++i) {
-            if (N % RS == 0 || cp0 + RS * i < N) {
-              float4 o = *reinterpret_cast<const float4*>(st + cso + RS * i * LPB);
-              float4* gp = reinterpret_cast<float4*>(g + (long long)RS * i * sstr);
+          for (int i = 0; i < (N + RO - 1) / RO; ++i) {
+            if (N % RO == 0 || r0 + RO * i < N) {
+              const float2 e0 = s0[RO * i], e1 = s0[RO * i + PS];
+              float4 o = make_float4(e0.x, e0.y, e1.x, e1.y);
+              float4* gp = reinterpret_cast<float4*>(g + (long long)RO * i * sstr);
               if (ACC && beta != 0.f) {
-                const float4 q = *gp;
-                o.x += beta * q.x;
-                o.y += beta * q.y;
-                o.z += beta * q.z;
-                o.w += beta * q.w;
+                const float4 w = *gp;
+                o.x += beta * w.x;
+                o.y += beta * w.y;
+                o.z += beta * w.z;
+                o.w += beta * w.w;
               }
               *gp = o;
             }
@@ -287,7 +297,6 @@ __global__ void __launch_bounds__(kThreads, ACC ? 2 : 3) pipe_kernel(LinePassArg
         }
       }
     }
-    __syncthreads();  // the buffer is free for the copy issued by the next item
     cur = nxt;
   }
   cp_async_wait_0();
