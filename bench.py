@@ -37,6 +37,11 @@ CFG = dict(N=(256, 256, 176), coils=32, coils_kept=16, shots=64, rot_deg=5.0, tr
 SMALL = dict(N=(64, 64, 48), coils=8, coils_kept=6, shots=16, rot_deg=5.0, trans_vox=3.0, snr_db=25.0,
              ellipsoids=12, seed=2001)
 NOMINAL_COUNTS = {"outer": [20, 20], "cg_final": 30}  # nominal schedule for the CPU reference estimate
+# DRAM bytes (read + write) per line-pass launch at 64 states: an ncu capture of
+# the strided and contiguous passes at 4 states (679.5 MB per launch, mean of
+# launches 2-4 of a forward transform) scaled by 16; stores still held in L2
+# when a launch ends are not counted.
+TRAFFIC_PER_LAUNCH = 10.87e9
 
 
 def peaks():
@@ -235,6 +240,51 @@ def cpu_estimate(N, n_states, C, counts, budget_note=True):
     return est, threads, desc
 
 
+# ---------------------------------------------------------------- transform only
+def transform_only(cfg, S, warmup, steps):
+    """Time the forward transform, the inverse without and with the state sum
+    of a random volume of the scan size with S random motion states, through
+    the C ABI with preallocated buffers (CUDA events, best of `steps` after
+    `warmup` calls). One JSON line; GB/s counts 11 passes of 16 bytes per
+    voxel and state."""
+    import disorder_b200 as db
+    from disorder_b200 import _lib, api, synth
+    N = tuple(cfg["N"])
+    rng = np.random.default_rng(0)
+    ctx = db.Context(0)
+    x = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    T = synth.motion(S, cfg["rot_deg"], cfg["trans_vox"], rng)
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    grids = db.generateTransformGrids(N, N, cent)
+    et, _ = db.precomputeFactorsSincRigidTransform(grids, T, 1)
+    plan = api._transform_plan(ctx, grids)
+    Tf = np.asfortranarray(et.T.astype(np.float32))
+    Tp = Tf.ctypes.data_as(_lib.FP)
+    V = int(np.prod(N))
+    xd = ctx.upload(x)
+    xs, xo, x1 = ctx.empty(N + (S,)), ctx.empty(N + (S,)), ctx.empty(N)
+    L = ctx.lib
+    calls = {
+        "forward": lambda: L.disorder_sinc_rigid_transform(ctx.h, plan.h, xd.ptr, 1, Tp, S, 1, 1, 1, xs.ptr),
+        "inverse": lambda: L.disorder_sinc_rigid_transform(ctx.h, plan.h, xs.ptr, S, Tp, S, 0, 0, 1, xo.ptr),
+        "inverse_sum": lambda: L.disorder_sinc_rigid_transform(ctx.h, plan.h, xs.ptr, S, Tp, S, 0, 1, 1, x1.ptr),
+    }
+    res = {}
+    for name, f in calls.items():
+        for _ in range(max(warmup, 1)):
+            ctx.check(f())
+        ctx.synchronize()
+        ts = []
+        for _ in range(max(steps, 1)):
+            ctx.event(0)
+            ctx.check(f())
+            ctx.event(1)
+            ts.append(ctx.elapsed_ms(0, 1))
+        t = min(ts)
+        res[name] = {"ms": t, "GB/s": 11 * 16.0 * V * S / (t * 1e-3) / 1e9}
+    print(json.dumps({"transform": "x".join(map(str, N)), "states": S, "launches": ctx.launches, "results": res}))
+
+
 # ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -244,8 +294,14 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--small", action="store_true", help="small scan (functional check)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--transform-only", type=int, default=0, metavar="STATES",
+                    help="only time the sinc rigid transform of the scan size with STATES states")
     args = ap.parse_args()
     cfg = SMALL if args.small else CFG
+    if args.transform_only:
+        return transform_only(cfg, args.transform_only, args.warmup, args.steps)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -298,12 +354,18 @@ def main():
     clk = ClockSampler(local)
     clk.start()
     l0 = ctx.launches
+    if args.profile_region:
+        import torch
+        torch.cuda.profiler.start()
     ctx.event(0)
     logs = []
     for _ in range(args.steps):
         x, T, log = one(sc.S, sc.y)
         logs.append(log)
     ctx.event(1)
+    if args.profile_region:
+        ctx.synchronize()
+        torch.cuda.profiler.stop()
     ms_total = ctx.elapsed_ms(0, 1)
     launches = ctx.launches - l0
     clocks = clk.stop()
@@ -339,25 +401,38 @@ def main():
     # and writing the 64 state volumes)
     N = cfg["N"]
     V = int(np.prod(N))
+    S = cfg["shots"]
     cent = [math.ceil((n + 1) / 2.0) for n in N]
-    et, _ = db.precomputeFactorsSincRigidTransform(db.generateTransformGrids(N, N, cent), sc.T_gt, 1)
-    xg = sc.x_gt
-    outt, _ = db.sincRigidTransform(xg, et, 1, ctx=ctx)
+    grids = db.generateTransformGrids(N, N, cent)
+    et, _ = db.precomputeFactorsSincRigidTransform(grids, sc.T_gt, 1)
+    from disorder_b200 import _lib, api
+    tplan = api._transform_plan(ctx, grids)
+    Tf = np.asfortranarray(et.T.astype(np.float32))
+    Tp = Tf.ctypes.data_as(_lib.FP)
+    xg = ctx.upload(sc.x_gt_host.astype(np.complex64))
+    outt = ctx.empty(tuple(N) + (S,))
+
+    def fwd():
+        ctx.check(ctx.lib.disorder_sinc_rigid_transform(ctx.h, tplan.h, xg.ptr, 1, Tp, S, 1, 1, 1, outt.ptr))
+
+    fwd()
     ctx.synchronize()
-    reps = 3
+    reps = 5
     ctx.event(4)
     for _ in range(reps):
-        outt, _ = db.sincRigidTransform(xg, et, 1, ctx=ctx)
+        fwd()
     ctx.event(5)
     t_fwd = ctx.elapsed_ms(4, 5) / reps
-    del outt
+    del outt, xg
     n_pass = 11
-    bytes_per_launch = 16.0 * V * cfg["shots"]
+    bytes_per_launch = 16.0 * V * S  # read + write of the 64 complex64 state volumes
     achieved = bytes_per_launch / (t_fwd / n_pass * 1e-3) / 1e9
     peak, pkind = peaks()
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "fp::line_kernel (sinc-transform line pass)",
-            "peak_kind": pkind, "bytes_per_launch": bytes_per_launch}
+            "traffic": TRAFFIC_PER_LAUNCH, "kernel": "fp::pipe_kernel (pipelined sinc-transform line pass)",
+            "peak_kind": pkind, "bytes_per_launch": bytes_per_launch,
+            "timing": "one forward transform (11 launches, phase-seed build included) through the C ABI, "
+                      "%d states, CUDA events, mean of %d" % (S, reps)}
 
     out = {"metric": METRIC, "value": ms * 1e-3 / world, "unit": "s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
