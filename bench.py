@@ -285,6 +285,60 @@ def transform_only(cfg, S, warmup, steps):
     print(json.dumps({"transform": "x".join(map(str, N)), "states": S, "launches": ctx.launches, "results": res}))
 
 
+# ---------------------------------------------------------------- operators only
+def operator_only(cfg, S, warmup, steps):
+    """Time encode, decode and encodedecode (the normal operator) of a random
+    volume of the scan size with the kept coil count, a random-checkered
+    sampling of S shots and S random motion states, through the C ABI with
+    preallocated buffers (CUDA events, best of `steps` after `warmup` calls).
+    One JSON line."""
+    import disorder_b200 as db
+    from disorder_b200 import _lib, api, synth
+    N = tuple(cfg["N"])
+    C = cfg["coils_kept"]
+    rng = np.random.default_rng(1)
+    ctx = db.Context(0)
+    x = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    Sf = np.empty(N + (C,), np.complex64)
+    for c in range(C):
+        Sf[..., c] = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    H = synth.random_checkered(N[:2], S, rng)
+    ky, kz, nEc, mSt, _ = synth.sample_lists(H, S)
+    T = synth.motion(S, cfg["rot_deg"], cfg["trans_vox"], rng)
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    Sd = ctx.upload(Sf)
+    del Sf
+    E = db.Struct(Tr=T, NMs=S, NSe=S + 1, Sf=Sd, grids=db.generateTransformGrids(N, N, cent), ky=ky, kz=kz,
+                  nEc=nEc, mSt=mSt)
+    plan = api._plan(E, ctx)
+    xd = ctx.upload(x)
+    out = ctx.empty(N)
+    n_samples = int(nEc[-1])
+    y = ctx.empty((n_samples, 1, N[2], C))
+    Tf = np.asfortranarray(np.asarray(T, np.float32))
+    Tp = Tf.ctypes.data_as(_lib.FP)
+    L = ctx.lib
+    calls = {
+        "encode": lambda: L.disorder_encode(ctx.h, plan.h, xd.ptr, Sd.ptr, C, Tp, y.ptr),
+        "decode": lambda: L.disorder_decode(ctx.h, plan.h, y.ptr, Sd.ptr, C, Tp, None, None, out.ptr),
+        "encodedecode": lambda: L.disorder_encodedecode(ctx.h, plan.h, xd.ptr, Sd.ptr, C, Tp, None, out.ptr),
+    }
+    res = {}
+    for name, f in calls.items():
+        for _ in range(max(warmup, 1)):
+            ctx.check(f())
+        ctx.synchronize()
+        ts = []
+        for _ in range(max(steps, 1)):
+            ctx.event(0)
+            ctx.check(f())
+            ctx.event(1)
+            ts.append(ctx.elapsed_ms(0, 1))
+        res[name] = {"ms": min(ts)}
+    print(json.dumps({"operators": "x".join(map(str, N)), "coils": C, "shots": S, "launches": ctx.launches,
+                      "results": res}))
+
+
 # ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -298,10 +352,14 @@ def main():
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--transform-only", type=int, default=0, metavar="STATES",
                     help="only time the sinc rigid transform of the scan size with STATES states")
+    ap.add_argument("--operator-only", type=int, default=0, metavar="SHOTS",
+                    help="only time encode / decode / encodedecode of the scan size with SHOTS shots")
     args = ap.parse_args()
     cfg = SMALL if args.small else CFG
     if args.transform_only:
         return transform_only(cfg, args.transform_only, args.warmup, args.steps)
+    if args.operator_only:
+        return operator_only(cfg, args.operator_only, args.warmup, args.steps)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

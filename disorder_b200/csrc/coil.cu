@@ -190,10 +190,10 @@ __global__ void __launch_bounds__(kThreads) fft2_weight_kernel(CoilArgs a, float
   float2* X = fft_tile(ba, bb, tw, plan, L, P, tid, nthr);
   float2* Xs = (X == ba) ? bb : ba;
   const int seg = a.d_slot_seg[slot];
-  const float* wm = wmap + (long long)seg * a.N2 * N1 + t.ky0;
+  const float* wm = wmap + ((long long)seg * N1 + t.ky0) * a.N2;
   for (int e = tid; e < n * L; e += nthr) {
     const int p = e / L, l = e - p * L;
-    const float w = l < t.nl ? wm[(long long)p * N1 + l] : 0.f;
+    const float w = l < t.nl ? wm[(long long)l * a.N2 + p] : 0.f;
     X[p * P + l] = cconj(cscale(X[p * P + l], w));
   }
   __syncthreads();
@@ -253,7 +253,7 @@ __global__ void weight_map_kernel(const int* __restrict__ segof, const int* __re
                                   int N1, int N2, float* __restrict__ wmap, float scale) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
     const float w = (We ? We[i] : 1.f) * scale;
-    atomicAdd(&wmap[((long long)segof[i] * N2 + kzv[i]) * N1 + kyv[i]], w);
+    atomicAdd(&wmap[((long long)segof[i] * N1 + kyv[i]) * N2 + kzv[i]], w);
   }
 }
 
@@ -351,8 +351,13 @@ int dis_coil_scatter_ifft2(disorder_ctx_s* ctx, const disorder_plan_s* plan, con
 int dis_coil_fft2_weight(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, float2* A,
                          const float* wmap) {
   if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
-  // the fast kernel applies w and the explicit inverse; the 1/(N1*N2) of the
+  // the fast kernels apply w and the explicit inverse; the 1/(N1*N2) of the
   // inverse DFTs is applied by the combine step
+  if (dis_use_fast() && dis_use_pipe() && dis_fast_wpipe(a.N2, a, A, wmap, plan->d_tw[1], ctx->stream)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   if (dis_use_fast() && dis_fast_axis1(a.N2, 1, a, A, nullptr, nullptr, 0, 0, 0, 1.f, wmap, nullptr, nullptr, plan,
                                        plan->d_tw[1], ctx->stream)) {
     dis_count(ctx);

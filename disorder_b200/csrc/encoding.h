@@ -34,7 +34,7 @@ struct EncodeDecodeSpec {
   const float* T = nullptr;
   int T_n = 0;
   std::vector<int> segs;
-  const float* wmap = nullptr;  // [seg][N2][N1] sample weights of each grid point (three-pass path)
+  const float* wmap = nullptr;  // [seg][N1][N2] (kz fastest) sample weights of each grid point (three-pass path)
   const float* We = nullptr;    // per-sample weights (plane path), NULL for 1
 };
 

@@ -5,17 +5,21 @@
 #include "pipepass.cuh"
 #include "plane.cuh"
 
-extern template struct fp::PipeLaunch<4, 4>;
-extern template struct fp::PipeLaunch<8, 4>;
-extern template struct fp::PipeLaunch<4, 11>;
-extern template struct fp::PipeLaunch<8, 8>;
-extern template struct fp::PipeLaunch<8, 11>;
-extern template struct fp::PipeLaunch<8, 12>;
-extern template struct fp::PipeLaunch<16, 8>;
-extern template struct fp::PipeLaunch<16, 10>;
-extern template struct fp::PipeLaunch<16, 11>;
-extern template struct fp::PipeLaunch<16, 12>;
-extern template struct fp::PipeLaunch<16, 16>;
+#define DIS_EXTERN_PIPE(F1, F2)                 \
+  extern template struct fp::PipeLaunch<F1, F2>; \
+  extern template struct fp::WPipeLaunch<F1, F2>;
+DIS_EXTERN_PIPE(4, 4)
+DIS_EXTERN_PIPE(8, 4)
+DIS_EXTERN_PIPE(4, 11)
+DIS_EXTERN_PIPE(8, 8)
+DIS_EXTERN_PIPE(8, 11)
+DIS_EXTERN_PIPE(8, 12)
+DIS_EXTERN_PIPE(16, 8)
+DIS_EXTERN_PIPE(16, 10)
+DIS_EXTERN_PIPE(16, 11)
+DIS_EXTERN_PIPE(16, 12)
+DIS_EXTERN_PIPE(16, 16)
+#undef DIS_EXTERN_PIPE
 
 extern template struct fp::Launch<4, 4>;
 extern template struct fp::Launch<8, 4>;
@@ -71,6 +75,23 @@ bool dis_fast_pipe(const LinePassArgs& a, const float2* tw, cudaStream_t s) {
     case 176: return fp::PipeLaunch<16, 11>::run(a, tw, s);
     case 192: return fp::PipeLaunch<16, 12>::run(a, tw, s);
     case 256: return fp::PipeLaunch<16, 16>::run(a, tw, s);
+    default: return false;
+  }
+}
+
+bool dis_fast_wpipe(int n, const CoilArgs& a, float2* A, const float* wmap, const float2* tw, cudaStream_t s) {
+  switch (n) {
+    case 16: return fp::WPipeLaunch<4, 4>::run(a, A, wmap, tw, s);
+    case 32: return fp::WPipeLaunch<8, 4>::run(a, A, wmap, tw, s);
+    case 44: return fp::WPipeLaunch<4, 11>::run(a, A, wmap, tw, s);
+    case 64: return fp::WPipeLaunch<8, 8>::run(a, A, wmap, tw, s);
+    case 88: return fp::WPipeLaunch<8, 11>::run(a, A, wmap, tw, s);
+    case 96: return fp::WPipeLaunch<8, 12>::run(a, A, wmap, tw, s);
+    case 128: return fp::WPipeLaunch<16, 8>::run(a, A, wmap, tw, s);
+    case 160: return fp::WPipeLaunch<16, 10>::run(a, A, wmap, tw, s);
+    case 176: return fp::WPipeLaunch<16, 11>::run(a, A, wmap, tw, s);
+    case 192: return fp::WPipeLaunch<16, 12>::run(a, A, wmap, tw, s);
+    case 256: return fp::WPipeLaunch<16, 16>::run(a, A, wmap, tw, s);
     default: return false;
   }
 }

@@ -282,12 +282,14 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(CoilArgs a, const floa
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
   ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
   const long long nlines = (long long)a.N2 * a.N3c;
-  const long long q = (long long)blockIdx.x * LPB + li;
+  // 1-D grid with the slot fastest: the CTAs of all slots of one tile run
+  // together and read that tile's coil-map lines once from HBM, then from L2
+  const int slot = (int)(blockIdx.x % a.n_slots);
+  const long long q = (long long)(blockIdx.x / a.n_slots) * LPB + li;
   const bool valid = q < nlines && lt < F2;
   const long long base = q * N;
   float2* myex = ex + li * LN::EXSZ;
   __syncthreads();
-  const int slot = blockIdx.y;
   const float2* zs = z + slot * a.Vz;
   float2 zr[F1];
 #pragma unroll
@@ -320,12 +322,13 @@ __global__ void __launch_bounds__(kThreads) combine_kernel(CoilArgs a, const flo
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
   ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
   const long long nlines = (long long)a.N2 * a.N3c;
-  const long long q = (long long)blockIdx.x * LPB + li;
+  // 1-D grid with the slot fastest (coil-map lines shared through L2)
+  const int slot = (int)(blockIdx.x % a.n_slots);
+  const long long q = (long long)(blockIdx.x / a.n_slots) * LPB + li;
   const bool ok = q < nlines;
   const long long base = q * N;
   float2* myex = ex + li * LN::EXSZ;
   __syncthreads();
-  const int slot = blockIdx.y;
   const long long Vc = nlines * N;
   float2 acc[F1];
 #pragma unroll
@@ -436,11 +439,11 @@ __global__ void __launch_bounds__(kThreads) axis1_kernel(CoilArgs a, float2* __r
     return;
   }
   if (MODE == 1) {
-    const float* wm = wmap + (long long)seg * N * N1 + t.ky0 + li;
+    const float* wm = wmap + ((long long)seg * N1 + t.ky0 + li) * N;
     if (lt < F1) {
 #pragma unroll
       for (int k2 = 0; k2 < F2; ++k2) {
-        const float w = li < t.nl ? wm[(long long)(lt + F1 * k2) * N1] : 0.f;
+        const float w = li < t.nl ? wm[lt + F1 * k2] : 0.f;
         X[k2] = cscale(X[k2], w);
       }
     }
@@ -499,14 +502,14 @@ struct Launch {
     static bool once = init();
     (void)once;
     const long long nl = (long long)a.N2 * a.N3c;
-    dim3 grid((unsigned)((nl + LPB - 1) / LPB), (unsigned)a.n_slots);
+    const unsigned grid = (unsigned)(((nl + LPB - 1) / LPB) * a.n_slots);
     expand_kernel<F1, F2><<<grid, kThreads, smem(false), s>>>(a, z, A, tw);
   }
   static void combine(const CoilArgs& a, const float2* A, float2* u, float scale, const float2* tw, cudaStream_t s) {
     static bool once = init();
     (void)once;
     const long long nl = (long long)a.N2 * a.N3c;
-    dim3 grid((unsigned)((nl + LPB - 1) / LPB), (unsigned)a.n_slots);
+    const unsigned grid = (unsigned)(((nl + LPB - 1) / LPB) * a.n_slots);
     combine_kernel<F1, F2><<<grid, kThreads, smem(false), s>>>(a, A, u, scale, tw);
   }
   static void axis1(int mode, const CoilArgs& a, float2* A, float2* y, const float2* ymeas, long long ld, int n3off,

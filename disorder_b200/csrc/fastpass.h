@@ -10,6 +10,9 @@ bool dis_fast_line(const LinePassArgs& a, const float2* tw, cudaStream_t s);
 // Pipelined persistent kernel (pipepass.cuh) for the single-input passes;
 // false when the pass does not fit it.
 bool dis_fast_pipe(const LinePassArgs& a, const float2* tw, cudaStream_t s);
+// Pipelined weighted dim-2 pass of the normal operator (pipepass.cuh,
+// wpipe_kernel) for line length n = N2; false when it does not apply.
+bool dis_fast_wpipe(int n, const CoilArgs& a, float2* A, const float* wmap, const float2* tw, cudaStream_t s);
 bool dis_fast_expand(int n, const CoilArgs& a, const float2* z, float2* A, const float2* tw, cudaStream_t s);
 bool dis_fast_combine(int n, const CoilArgs& a, const float2* A, float2* u, float scale, const float2* tw,
                       cudaStream_t s);

@@ -363,6 +363,143 @@ struct PipeLaunch {
   }
 };
 
+// ---------------------------------------------------------------- weighted pass of the normal operator
+// A[slot][c] <- IFFT_2(w_seg .* FFT_2(A[slot][c])) in place (unnormalised;
+// the combine step applies the scale), the dim-2 step of encodedecode on the
+// per-coil intermediates of an N1 x N2 x N3c slab (ky fastest). w_seg is the
+// segment's sample-weight map wmap[seg][ky][kz]. Work unit = (tile of LPB ky
+// rows at one readout position, slot); the CTA walks the unit's C coils with
+// the same double-buffered pipeline as pipe_kernel (strided layout), so the
+// unit's weights come from L1 after its first coil.
+template <int F1, int F2>
+__global__ void __launch_bounds__(kThreads, 3) wpipe_kernel(CoilArgs a, float2* __restrict__ A,
+                                                            const float* __restrict__ wmap,
+                                                            const float2* __restrict__ twg, int n_tiles) {
+  using P = Pipe<F1, F2>;
+  using LN = typename P::LN;
+  constexpr int N = P::N, TL = P::TL, LPB = P::LPB, SB = P::SB, PS = P::PS, RS = P::RS;
+  extern __shared__ __align__(16) float2 sm[];
+  float2* tw = sm;
+  float2* stg = sm + P::TW;
+  const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
+  ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
+  const int Nv[3] = {a.N1, a.N2, a.N3c};
+  const int S = a.n_slots, C = a.C, G = gridDim.x, b = blockIdx.x;
+  const int sstr = a.N1;
+  const long long Vc = (long long)a.N1 * a.N2 * a.N3c;
+  // units u = b + i*G < n_tiles*S (tile u / S, slot u % S), C items each
+  const int nu = n_tiles * S;
+  const int n_items = b < nu ? ((nu - 1 - b) / G + 1) * C : 0;
+  if (n_items == 0) return;
+  const int gq = G / S, gr = G % S;
+  auto unit_item = [&](int tile, int slot) { return pitem(Nv, 1, LPB, tile, slot); };
+  auto vol = [&](const PItem& it, int c) { return A + ((long long)it.slot * C + c) * Vc + it.base; };
+  const int sl = tid % LPB, sp0 = tid / LPB;
+  auto issue = [&](const PItem& it, int c, float2* st) {
+    if (sl < it.nv) {
+      const float2* g = vol(it, c) + sl + sp0 * sstr;
+      float2* d = st + sl * PS + sp0;
+#pragma unroll
+      for (int i = 0; i < P::SWEEPS; ++i)
+        if (N % RS == 0 || sp0 + RS * i < N) cp_async8(d + RS * i, g + (long long)RS * i * sstr);
+    }
+  };
+  PItem cur = unit_item(b / S, b % S);
+  int cc = 0;
+  issue(cur, 0, stg);
+  cp_async_commit();
+  for (int j = 0; j < n_items; ++j) {
+    float2* st = stg + (j & 1) * SB;
+    const bool valid = li < cur.nv;
+    // the line's weights w[seg][ky = ca + li][kz] (the same for all C coils of
+    // the unit, so read from L1 after the first coil)
+    const float* wm = wmap + ((long long)a.d_slot_seg[cur.slot] * a.N1 + cur.ca + (valid ? li : 0)) * a.N2;
+    cp_async_wait_0();
+    __syncthreads();  // item j staged; every thread is past item j-1
+    PItem nxt = cur;
+    int cn = cc + 1;
+    if (j + 1 < n_items) {
+      if (cn == C) {
+        cn = 0;
+        int slot = cur.slot + gr, tile = cur.tile + gq;
+        if (slot >= S) {
+          slot -= S;
+          ++tile;
+        }
+        nxt = unit_item(tile, slot);
+      }
+      issue(nxt, cn, stg + ((j + 1) & 1) * SB);
+    }
+    cp_async_commit();
+    float2* my = st + li * PS;
+    float2 v[F1], X[F2];
+#pragma unroll
+    for (int m = 0; m < F1; ++m) v[m] = (lt < F2 && valid) ? my[lt + F2 * m] : make_float2(0.f, 0.f);
+    __syncwarp();  // the line's span becomes its exchange area
+    LN::fwd(v, X, lt, my, tw);
+    if (lt < F1) {
+#pragma unroll
+      for (int k2 = 0; k2 < F2; ++k2) X[k2] = cscale(X[k2], wm[lt + F1 * k2]);
+    }
+    LN::inv(X, v, lt, my, tw);
+    if (lt < F2) {
+#pragma unroll
+      for (int m = 0; m < F1; ++m) my[lt + F2 * m] = v[m];
+    }
+    __syncthreads();
+    constexpr int PPR = LPB / 2, RO = kThreads / PPR;  // line pairs per row, rows per sweep
+    const int q = tid % PPR, r0 = tid / PPR;
+    if (2 * q < cur.nv) {  // nv is even: N1 is even and tiles start at multiples of LPB
+      const float2* s0 = st + 2 * q * PS + r0;
+      float2* g = vol(cur, cc) + 2 * q + (long long)r0 * sstr;
+#pragma unroll
+      for (int i = 0; i < (N + RO - 1) / RO; ++i) {
+        if (N % RO == 0 || r0 + RO * i < N) {
+          const float2 e0 = s0[RO * i], e1 = s0[RO * i + PS];
+          *reinterpret_cast<float4*>(g + (long long)RO * i * sstr) = make_float4(e0.x, e0.y, e1.x, e1.y);
+        }
+      }
+    }
+    cur = nxt;
+    cc = cn;
+  }
+  cp_async_wait_0();
+}
+
+template <int F1, int F2>
+struct WPipeLaunch {
+  using P = Pipe<F1, F2>;
+  struct Occ {
+    int per_sm = 0, sms = 0;
+  };
+  static Occ init() {
+    Occ o;
+    cudaFuncSetAttribute(wpipe_kernel<F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, wpipe_kernel<F1, F2>, kThreads, P::SMEM);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev);
+    return o;
+  }
+  // false when the slab does not fit this kernel (odd N1, unaligned A,
+  // 2^31 or more units)
+  static bool run(const CoilArgs& a, float2* A, const float* wmap, const float2* tw, cudaStream_t s) {
+    static const Occ occ = init();
+    if (occ.per_sm <= 0 || occ.sms <= 0) return false;
+    if ((a.N1 & 1) || (reinterpret_cast<uintptr_t>(A) & 15)) return false;
+    if ((long long)a.N1 * a.N2 * a.N3c >= (1LL << 31)) return false;
+    const long long tiles = (long long)((a.N1 + P::LPB - 1) / P::LPB) * a.N3c;
+    const long long units = tiles * a.n_slots;
+    if (units == 0 || units * a.C >= (1LL << 31)) return false;
+    const long long cap = (long long)occ.sms * occ.per_sm;
+    const unsigned grid = (unsigned)(units < cap ? units : cap);
+    wpipe_kernel<F1, F2><<<grid, kThreads, P::SMEM, s>>>(a, A, wmap, tw, (int)tiles);
+    return true;
+  }
+};
+
 }  // namespace fp
 
-#define DIS_PIPE_INSTANTIATE(F1, F2) template struct fp::PipeLaunch<F1, F2>;
+#define DIS_PIPE_INSTANTIATE(F1, F2) \
+  template struct fp::PipeLaunch<F1, F2>; \
+  template struct fp::WPipeLaunch<F1, F2>;
