@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -64,6 +65,14 @@ int dis_small(disorder_ctx_s* ctx, Workspace* ws) {
   return DISORDER_OK;
 }
 
+static bool use_pool() {
+  static const bool v = [] {
+    const char* e = std::getenv("DISORDER_POOL");
+    return !(e && e[0] == '0');
+  }();
+  return v;
+}
+
 #define CTX_CHECK(ctx) \
   if (!(ctx)) return DISORDER_BAD_ARG
 #define DEV_GUARD(ctx) DIS_CUDA_TRY(cudaSetDevice((ctx)->device))
@@ -93,6 +102,14 @@ int disorder_ctx_create(int device, disorder_ctx* out) {
     return DISORDER_CUDA_ERR;
   }
   ctx->own_stream = true;
+  // keep memory freed to the device's default pool (disorder_free) cached
+  // for reuse instead of returning it to the driver at each synchronisation
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   *out = ctx;
   return DISORDER_OK;
 }
@@ -141,10 +158,13 @@ int disorder_malloc(disorder_ctx ctx, size_t bytes, void** dptr) {
   CTX_CHECK(ctx);
   if (!dptr) return dis_set_error(ctx, DISORDER_BAD_ARG, "malloc: null output");
   DEV_GUARD(ctx);
-  cudaError_t e = cudaMalloc(dptr, std::max<size_t>(bytes, 1));
+  // stream-ordered: no device-wide synchronisation, pooled reuse
+  // (DISORDER_POOL=0: plain cudaMalloc / cudaFree)
+  cudaError_t e = use_pool() ? cudaMallocAsync(dptr, std::max<size_t>(bytes, 1), ctx->stream)
+                             : cudaMalloc(dptr, std::max<size_t>(bytes, 1));
   if (e != cudaSuccess) {
     cudaGetLastError();
-    return dis_set_error(ctx, DISORDER_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    return dis_set_error(ctx, DISORDER_OOM, "cudaMallocAsync(%zu): %s", bytes, cudaGetErrorString(e));
   }
   return DISORDER_OK;
 }
@@ -152,8 +172,13 @@ int disorder_malloc(disorder_ctx ctx, size_t bytes, void** dptr) {
 int disorder_free(disorder_ctx ctx, void* dptr) {
   CTX_CHECK(ctx);
   DEV_GUARD(ctx);
-  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  DIS_CUDA_TRY(cudaFree(dptr));
+  if (!dptr) return DISORDER_OK;
+  if (use_pool()) {
+    DIS_CUDA_TRY(cudaFreeAsync(dptr, ctx->stream));
+  } else {
+    DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    DIS_CUDA_TRY(cudaFree(dptr));
+  }
   return DISORDER_OK;
 }
 

@@ -52,6 +52,10 @@ const char* disorder_last_error(disorder_ctx ctx);
 int disorder_ctx_set_stream(disorder_ctx ctx, void* cuda_stream); /* NULL: own stream */
 void* disorder_ctx_get_stream(disorder_ctx ctx);
 int disorder_synchronize(disorder_ctx ctx);
+/* Device memory from the device's stream-ordered pool: usable by work on the
+ * context's stream at once, and by host code after disorder_synchronize.
+ * disorder_free returns it in stream order without waiting; the pool keeps
+ * freed memory for reuse until the process exits. */
 int disorder_malloc(disorder_ctx ctx, size_t bytes, void** dptr);
 int disorder_free(disorder_ctx ctx, void* dptr);
 int disorder_memcpy_h2d(disorder_ctx ctx, void* dst, const void* src, size_t bytes);
