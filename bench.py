@@ -348,7 +348,7 @@ def transform_only(cfg, S, warmup, steps):
 
 
 # ---------------------------------------------------------------- operators only
-def operator_only(cfg, S, warmup, steps):
+def operator_only(cfg, S, warmup, steps, profile_region=False):
     """Time encode, decode and encodedecode (the normal operator) of a random
     volume of the scan size with the kept coil count, a random-checkered
     sampling of S shots and S random motion states, through the C ABI with
@@ -397,6 +397,13 @@ def operator_only(cfg, S, warmup, steps):
             ctx.event(1)
             ts.append(ctx.elapsed_ms(0, 1))
         res[name] = {"ms": min(ts)}
+    if profile_region:  # one more encodedecode between cudaProfilerStart/Stop
+        import torch
+        ctx.synchronize()
+        torch.cuda.profiler.start()
+        ctx.check(calls["encodedecode"]())
+        ctx.synchronize()
+        torch.cuda.profiler.stop()
     print(json.dumps({"operators": "x".join(map(str, N)), "coils": C, "shots": S, "launches": ctx.launches,
                       "results": res}))
 
@@ -421,7 +428,7 @@ def main():
     if args.transform_only:
         return transform_only(cfg, args.transform_only, args.warmup, args.steps)
     if args.operator_only:
-        return operator_only(cfg, args.operator_only, args.warmup, args.steps)
+        return operator_only(cfg, args.operator_only, args.warmup, args.steps, args.profile_region)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

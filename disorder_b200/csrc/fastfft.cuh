@@ -261,18 +261,18 @@ struct DFT<9, INV> : DFT2D<3, 3, INV> {};
 
 // ---------------------------------------------------------------- twiddles
 // Shared-memory twiddles of a line FFT of length N = N1*N2 (SIZE float2):
-//   [k1*P + t]     W_N^{t k1}  (k1 < N1, t < N2): the four-step twiddles
-//   [W1 + q]       W_N1^q      (q < N1): the N1-point DFTs
-//   [W2 + q]       W_N2^q      (q < N2): the N2-point DFTs
-// The row pitch P is odd, so that the forward reads (fixed k1, consecutive t
-// across the lanes) and the inverse reads (fixed t, consecutive k1 across the
-// lanes, stride P) both hit 16 distinct 8-byte bank pairs.
+//   [t*Q + k] = W_N^{t k}   (t, k < M = max(N1, N2))
+// The forward step reads row t (its lane) at k = k1 and the inverse step row
+// t at k = u, two entries per 16-byte load. The row pitch Q is twice an odd
+// number, so 16 lanes reading the same column pair of their own rows hit the
+// minimum two wavefronts. P is the (odd) pitch of the exchange tiles.
 template <int N1, int N2>
 struct Tw {
+  static constexpr int M = N1 > N2 ? N1 : N2;
+  static constexpr int Q0 = (M + 1) & ~1;
+  static constexpr int Q = ((Q0 / 2) % 2 == 1) ? Q0 : Q0 + 2;
+  static constexpr int SIZE = M * Q;
   static constexpr int P = (N2 % 2 == 0) ? N2 + 1 : N2 + 2;
-  static constexpr int W1 = N1 * P;
-  static constexpr int W2 = W1 + N1;
-  static constexpr int SIZE = (W2 + N2 + 1) & ~1;
 };
 
 // Fill the table above from the N-point table twg[m] = W_N^m (global memory).
@@ -281,16 +281,8 @@ DIS_D void load_tw(float2* tws, const float2* __restrict__ twg, int tid, int nth
   using T = Tw<N1, N2>;
   constexpr int N = N1 * N2;
   for (int e = tid; e < T::SIZE; e += nthr) {
-    float2 v = make_float2(0.f, 0.f);
-    if (e < T::W1) {
-      const int k1 = e / T::P, t = e % T::P;
-      if (t < N2) v = twg[(t * k1) % N];
-    } else if (e < T::W2) {
-      v = twg[(e - T::W1) * N2];
-    } else if (e < T::W2 + N2) {
-      v = twg[(e - T::W2) * N1];
-    }
-    tws[e] = v;
+    const int t = e / T::Q, k = e % T::Q;
+    tws[e] = k < T::M ? twg[(t * k) % N] : make_float2(0.f, 0.f);
   }
 }
 
@@ -308,10 +300,16 @@ struct Line {
   // A -> B. a: layout A (used when t < N2); c: layout B (valid when t < N1)
   static DIS_D void fwd(float2 (&a)[N1], float2 (&c)[N2], int t, float2* ex, const float2* tw) {
     using T = Tw<N1, N2>;
+    static_assert(N1 % 2 == 0, "paired twiddle loads");
     if (t < N2) {
-      DFT<N1, false>::run(a, tw + T::W1, 1);
+      DFT<N1, false>::run(a, nullptr, 1);
+      const float4* tr = reinterpret_cast<const float4*>(tw + t * T::Q);
 #pragma unroll
-      for (int k1 = 1; k1 < N1; ++k1) a[k1] = cmul(a[k1], tw[k1 * T::P + t]);
+      for (int j = 0; j < N1 / 2; ++j) {
+        const float4 w = tr[j];
+        if (j > 0) a[2 * j] = cmul(a[2 * j], make_float2(w.x, w.y));
+        a[2 * j + 1] = cmul(a[2 * j + 1], make_float2(w.z, w.w));
+      }
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) ex[k1 * EX + t] = a[k1];
     }
@@ -319,7 +317,7 @@ struct Line {
     if (t < N1) {
 #pragma unroll
       for (int u = 0; u < N2; ++u) c[u] = ex[t * EX + u];
-      DFT<N2, false>::run(c, tw + T::W2, 1);
+      DFT<N2, false>::run(c, nullptr, 1);
     }
     __syncwarp();
   }
@@ -328,9 +326,14 @@ struct Line {
   static DIS_D void inv(float2 (&c)[N2], float2 (&a)[N1], int t, float2* ex, const float2* tw) {
     using T = Tw<N1, N2>;
     if (t < N1) {
-      DFT<N2, true>::run(c, tw + T::W2, 1);
+      DFT<N2, true>::run(c, nullptr, 1);
+      const float4* tr = reinterpret_cast<const float4*>(tw + t * T::Q);
 #pragma unroll
-      for (int u = 1; u < N2; ++u) c[u] = cmulc(c[u], tw[t * T::P + u]);
+      for (int j = 0; j < (N2 + 1) / 2; ++j) {
+        const float4 w = tr[j];
+        if (j > 0) c[2 * j] = cmulc(c[2 * j], make_float2(w.x, w.y));
+        if (2 * j + 1 < N2) c[2 * j + 1] = cmulc(c[2 * j + 1], make_float2(w.z, w.w));
+      }
 #pragma unroll
       for (int u = 0; u < N2; ++u) ex[t * EX + u] = c[u];
     }
@@ -338,7 +341,7 @@ struct Line {
     if (t < N2) {
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) a[k1] = ex[k1 * EX + t];
-      DFT<N1, true>::run(a, tw + T::W1, 1);
+      DFT<N1, true>::run(a, nullptr, 1);
     }
     __syncwarp();
   }

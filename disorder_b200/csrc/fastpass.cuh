@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kThreads) line_kernel(LinePassArgs a, const fl
   constexpr bool DUAL = (MODE & 1) != 0, ACC = (MODE & 2) != 0;
   using LN = ff::Line<F1, F2>;
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   float2* tw = sm;
   float2* ex = sm + LN::TWS;
   float2* st = ex + LPB * LN::EXSZ;
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(CoilArgs a, const floa
                                                           float2* __restrict__ A, const float2* __restrict__ twg) {
   using LN = ff::Line<F1, F2>;
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   float2* tw = sm;
   float2* ex = sm + LN::TWS;
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(kThreads) combine_kernel(CoilArgs a, const flo
                                                            const float2* __restrict__ twg) {
   using LN = ff::Line<F1, F2>;
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   float2* tw = sm;
   float2* ex = sm + LN::TWS;
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(kThreads) axis1_kernel(CoilArgs a, float2* __r
                                                          const int* __restrict__ kzv, const float2* __restrict__ twg) {
   using LN = ff::Line<F1, F2>;
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL, P = LPB + 1;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   float2* tw = sm;
   float2* ex = sm + LN::TWS;
   float2* st = ex + LPB * LN::EXSZ;

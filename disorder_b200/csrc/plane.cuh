@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(kThreads) plane_kernel(PlaneArgs a, const floa
   using LY = Layout<F1, F2>;
   using LN = typename LY::LN;
   constexpr int N1 = LY::N1, TL = LY::TL, CB = LY::CB, XP = LY::XP;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   const int N2 = a.N2;
   float2* tw1 = sm;
   float2* tw2 = tw1 + LN::TWS;
