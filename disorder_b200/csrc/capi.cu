@@ -110,6 +110,13 @@ int disorder_ctx_create(int device, disorder_ctx* out) {
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
   cudaGetLastError();
+  if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess || cudaMemset(ctx->d_err, 0, 256) != cudaSuccess) {
+    cudaGetLastError();
+    if (ctx->d_err) cudaFree(ctx->d_err);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return DISORDER_OOM;
+  }
   *out = ctx;
   return DISORDER_OK;
 }
@@ -121,6 +128,7 @@ int disorder_ctx_destroy(disorder_ctx ctx) {
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->ws2) cudaFree(ctx->ws2);
   if (ctx->small) cudaFree(ctx->small);
+  if (ctx->d_err) cudaFree(ctx->d_err);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -151,6 +159,13 @@ int disorder_synchronize(disorder_ctx ctx) {
   CTX_CHECK(ctx);
   DEV_GUARD(ctx);
   DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  // a bounded in-kernel wait that ran out (the kernel stopped early)
+  int err = 0;
+  DIS_CUDA_TRY(cudaMemcpy(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    DIS_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(int)));
+    return dis_set_error(ctx, DISORDER_TIMEOUT, "a TMA tile wait in a line pass ran out; results are incomplete");
+  }
   return DISORDER_OK;
 }
 

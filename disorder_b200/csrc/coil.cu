@@ -353,6 +353,11 @@ int dis_coil_fft2_weight(disorder_ctx_s* ctx, const disorder_plan_s* plan, const
   if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
   // the fast kernels apply w and the explicit inverse; the 1/(N1*N2) of the
   // inverse DFTs is applied by the combine step
+  if (dis_use_fast() && dis_use_pipe() && dis_fast_tma_weight(ctx, a, A, wmap, plan->d_tw[1])) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   if (dis_use_fast() && dis_use_pipe() && dis_fast_wpipe(a.N2, a, A, wmap, plan->d_tw[1], ctx->stream)) {
     dis_count(ctx);
     DIS_CUDA_TRY(cudaGetLastError());

@@ -13,6 +13,10 @@ bool dis_fast_pipe(const LinePassArgs& a, const float2* tw, cudaStream_t s);
 // Pipelined weighted dim-2 pass of the normal operator (pipepass.cuh,
 // wpipe_kernel) for line length n = N2; false when it does not apply.
 bool dis_fast_wpipe(int n, const CoilArgs& a, float2* A, const float* wmap, const float2* tw, cudaStream_t s);
+// TMA tile-copy variants (tmapass.cuh) of the strided transform passes and
+// of the weighted pass; false when the pass does not fit them.
+bool dis_fast_tma_line(disorder_ctx_s* ctx, const LinePassArgs& a);
+bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, const float* wmap, const float2* tw);
 bool dis_fast_expand(int n, const CoilArgs& a, const float2* z, float2* A, const float2* tw, cudaStream_t s);
 bool dis_fast_combine(int n, const CoilArgs& a, const float2* A, float2* u, float scale, const float2* tw,
                       cudaStream_t s);

@@ -25,6 +25,7 @@ struct disorder_ctx_s {
   void* small = nullptr;
   size_t small_bytes = 0;
   cudaEvent_t ev[16] = {};
+  int* d_err = nullptr;  // device error word of bounded in-kernel waits (0: none)
 };
 
 // Workspace bump allocator on top of the context's cached buffer.

@@ -248,6 +248,11 @@ int dis_line_pass(disorder_ctx_s* ctx, LinePassArgs a) {
   const int n = a.N[a.axis];
   if (a.plan.n != n) return dis_set_error(ctx, DISORDER_BAD_ARG, "line pass: plan size %d != axis size %d", a.plan.n, n);
   if (a.n_slots == 0) return DISORDER_OK;
+  if (dis_use_fast() && a.tw && dis_use_pipe() && dis_fast_tma_line(ctx, a)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   if (dis_use_fast() && a.tw && dis_use_pipe() && dis_fast_pipe(a, a.tw, ctx->stream)) {
     dis_count(ctx);
     DIS_CUDA_TRY(cudaGetLastError());
