@@ -506,6 +506,13 @@ def main():
         ms = float(t.item())
     err = nrmse(ctx, x, sc.x_gt_host)
     motion_err = float(np.max(np.abs(T - sc.T_gt)[:, :3])), float(np.degrees(np.max(np.abs(T - sc.T_gt)[:, 3:])))
+    # host-side phase durations of the last timed reconstruction (the solver
+    # calls synchronise, so these include their GPU time)
+    phases, prev = {}, 0.0
+    for e in logs[-1].events:
+        key = e["step"] + ("_L%d" % e["level"] if "level" in e else "")
+        phases[key] = phases.get(key, 0.0) + (e["t"] - prev)
+        prev = e["t"]
     counts = {"outer": [sum(1 for e in logs[-1].events if e["step"] == "lm" and e["level"] == lv) for lv in (0, 1)],
               "cg_final": sum(e["iters"] for e in logs[-1].events if e["step"] == "cg" and e["level"] == 2)}
 
@@ -575,7 +582,8 @@ def main():
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
            "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic", "config": config,
            "nrmse": err, "motion_max_err": {"trans_vox": motion_err[0], "rot_deg": motion_err[1]},
-           "schedule": counts, "gpu_launches": int(launches / args.steps), "clocks": clocks,
+           "schedule": counts, "phases_s": {k: round(v, 4) for k, v in phases.items()},
+           "gpu_launches": int(launches / args.steps), "clocks": clocks,
            "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": int(Sh.nbytes + yh.nbytes),
                    "d2h_bytes_per_step": int(V * 8)},
            "roofline": roof}

@@ -308,6 +308,12 @@ int dis_coil_expand_fft1(disorder_ctx_s* ctx, const disorder_plan_s* plan, const
 int dis_coil_fft2_gather(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* A,
                          float2* y, long long y_ld, int y_n3off, int y_N3, const float2* y_meas, float scale) {
   if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
+  if (dis_use_fast() && dis_use_pipe() &&
+      dis_fast_tma_gather(ctx, plan, a, A, y, y_ld, y_n3off, y_N3, y_meas, scale)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   if (dis_use_fast() && dis_fast_axis1(a.N2, 0, a, const_cast<float2*>(A), y, y_meas, y_ld, y_n3off, y_N3, scale,
                                        nullptr, nullptr, nullptr, plan, plan->d_tw[1], ctx->stream)) {
     dis_count(ctx);
@@ -330,6 +336,11 @@ int dis_coil_fft2_gather(disorder_ctx_s* ctx, const disorder_plan_s* plan, const
 int dis_coil_scatter_ifft2(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* y,
                            long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* A) {
   if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
+  if (dis_use_fast() && dis_use_pipe() && dis_fast_tma_scatter(ctx, plan, a, y, y_ld, y_n3off, y_N3, We, Mb, A)) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   if (dis_use_fast() && dis_fast_axis1(a.N2, 2, a, A, const_cast<float2*>(y), nullptr, y_ld, y_n3off, y_N3, 1.f,
                                        nullptr, We, Mb, plan, plan->d_tw[1], ctx->stream)) {
     dis_count(ctx);

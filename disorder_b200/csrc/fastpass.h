@@ -17,6 +17,10 @@ bool dis_fast_wpipe(int n, const CoilArgs& a, float2* A, const float* wmap, cons
 // of the weighted pass; false when the pass does not fit them.
 bool dis_fast_tma_line(disorder_ctx_s* ctx, const LinePassArgs& a);
 bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, const float* wmap, const float2* tw);
+bool dis_fast_tma_gather(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* A,
+                         float2* y, long long y_ld, int y_n3off, int y_N3, const float2* y_meas, float scale);
+bool dis_fast_tma_scatter(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* y,
+                          long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* A);
 bool dis_fast_expand(int n, const CoilArgs& a, const float2* z, float2* A, const float2* tw, cudaStream_t s);
 bool dis_fast_combine(int n, const CoilArgs& a, const float2* A, float2* u, float scale, const float2* tw,
                       cudaStream_t s);

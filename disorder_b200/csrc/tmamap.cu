@@ -126,3 +126,52 @@ bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, cons
   t.err = ctx->d_err;
   return launch_size(a.N2, 1, m, m, t, tw, 0, ctx->stream);
 }
+
+namespace {
+bool coil_tma(disorder_ctx_s* ctx, int kind, const CoilArgs& a, float2* A, const disorder_plan_s* plan,
+              fp::TArgs& t) {
+  if (!tma_enabled() || !ctx->d_err || !has_tma_size(a.N2)) return false;
+  const int Nv[3] = {a.N1, a.N2, a.N3c};
+  const long long Vc = (long long)a.N1 * a.N2 * a.N3c;
+  const long long nvol = (long long)a.n_slots * a.C;
+  if (nvol < 1 || nvol >= (1LL << 31)) return false;
+  CUtensorMap m;
+  if (!dis_tmap_volumes(&m, A, Nv, 1, Vc, (int)nvol)) return false;
+  for (int i = 0; i < 3; ++i) t.Nv[i] = Nv[i];
+  t.axis = 1;
+  t.n_vol = (int)nvol;
+  t.n_slots = a.n_slots;
+  t.C = a.C;
+  t.slot_seg = a.d_slot_seg;
+  t.err = ctx->d_err;
+  t.rowptr = plan->d_rowptr;
+  t.perm = plan->d_perm;
+  t.kyv = plan->d_ky;
+  t.kzv = plan->d_kz;
+  return launch_size(a.N2, kind, m, m, t, plan->d_tw[1], 0, ctx->stream);
+}
+}  // namespace
+
+bool dis_fast_tma_gather(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* A,
+                         float2* y, long long y_ld, int y_n3off, int y_N3, const float2* y_meas, float scale) {
+  fp::TArgs t = fp::TArgs();
+  t.y = y;
+  t.ymeas = y_meas;
+  t.ld = y_ld;
+  t.n3off = y_n3off;
+  t.N3y = y_N3;
+  t.scale = scale;
+  return coil_tma(ctx, 2, a, const_cast<float2*>(A), plan, t);
+}
+
+bool dis_fast_tma_scatter(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* y,
+                          long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* A) {
+  fp::TArgs t = fp::TArgs();
+  t.y = const_cast<float2*>(y);
+  t.ld = y_ld;
+  t.n3off = y_n3off;
+  t.N3y = y_N3;
+  t.We = We;
+  t.Mb = Mb;
+  return coil_tma(ctx, 3, a, A, plan, t);
+}

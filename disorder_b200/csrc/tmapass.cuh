@@ -84,7 +84,12 @@ struct TPipe {
 
 // KIND 0: transform pass (coefficient from the line's phase seeds, a.Sd);
 // KIND 1: normal-operator weighting (coefficient = sample weight, volumes are
-// the per-coil intermediates, unit = (tile, slot) walking its C coils).
+// the per-coil intermediates, unit = (tile, slot) walking its C coils);
+// KIND 2: encode gather (DFT along dim 2, then the segment's samples of the
+// tile's ky rows are read out of the tile into y; no store);
+// KIND 3: decode scatter (the tile is built from the weighted samples, then
+// the inverse DFT along dim 2 is stored; no load). Kinds 1-3 share the unit
+// walk over (tile, slot) and its C coils.
 // Geometry: volumes of Nv = {N0, N1, N2} with the pass along `axis` (1 or 2);
 // tile = 16 lines adjacent along N0 at one position of the other axis.
 struct TArgs {
@@ -96,6 +101,19 @@ struct TArgs {
   const float* wmap;  // KIND 1: [seg][N0][N_pass]
   LinePassArgs a;     // KIND 0: seeds
   int* err;           // device error word (set to 1 when a wait runs out)
+  // KIND 2 / 3: per-segment CSR of the samples by ky row, sample rows and
+  // the sample array y[ld*(n3 + n3off) + ld*N3y*c + i]
+  const int* rowptr;
+  const int* perm;
+  const int* kyv;
+  const int* kzv;
+  float2* y;
+  const float2* ymeas;  // KIND 2: subtracted when non-null
+  long long ld;
+  int n3off, N3y;
+  float scale;          // KIND 2
+  const float* We;      // KIND 3: per-sample weights or null
+  const float* Mb;      // KIND 3: readout weights or null
 };
 
 template <int F1, int F2, int KIND>
@@ -122,7 +140,8 @@ __global__ void __launch_bounds__(kThreads, 3)
   }
   __syncthreads();
   const int G = gridDim.x, b = blockIdx.x;
-  const int S = KIND == 1 ? t.n_slots : t.n_vol, C = KIND == 1 ? t.C : 1;
+  constexpr bool LOAD = KIND != 3, STORE = KIND != 2;
+  const int S = KIND >= 1 ? t.n_slots : t.n_vol, C = KIND >= 1 ? t.C : 1;
   const int nu = n_tiles * S;  // units: tile u / S, slot u % S
   const int n_items = b < nu ? ((nu - 1 - b) / G + 1) * C : 0;
   if (n_items == 0) return;
@@ -137,13 +156,13 @@ __global__ void __launch_bounds__(kThreads, 3)
   };
   auto issue = [&](const PItem& it, int c, float2* st, uint64_t* bar) {
     mbar_expect_tx(bar, P::BOX_BYTES);
-    const int w = KIND == 1 ? it.slot * C + c : (shared_input ? 0 : it.slot);
+    const int w = KIND >= 1 ? it.slot * C + c : (shared_input ? 0 : it.slot);
     tma_load_tile(st, &in_map, it.ca, t.axis == 2 ? it.cb : 0, t.axis == 1 ? it.cb : 0, w, bar);
   };
   PItem cur;
   unit(b / S, b % S, cur);
   int cc = 0;
-  if (tid == 0) issue(cur, 0, stg0, &mbar[0]);
+  if (LOAD && tid == 0) issue(cur, 0, stg0, &mbar[0]);
   for (int j = 0; j < n_items; ++j) {
     float2* st = (j & 1) ? stg1 : stg0;
     const bool valid = li < cur.nv;
@@ -163,7 +182,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     // bounded wait for the tile (each try_wait suspends for a short
     // hardware-defined time; the bound is of the order of a second)
     bool late = false;
-    {
+    if (LOAD) {
       uint32_t spins = 0;
       while (!mbar_try_wait(&mbar[j & 1], (uint32_t)((j >> 1) & 1))) {
         if (++spins > (1u << 20)) {
@@ -192,17 +211,65 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
         unit(tile, slot, nxt);
       }
-      if (tid == 0) {
-        bulk_wait_read0();  // item j-1's store has read the other buffer
+      if (LOAD && tid == 0) {
+        if (STORE) bulk_wait_read0();  // item j-1's store has read the other buffer
         fence_async_smem();
         issue(nxt, cn, (j & 1) ? stg0 : stg1, &mbar[(j + 1) & 1]);
       }
     }
     float2 v[F1], X[F2];
+    float2* myex = st + li * LN::EXSZ;
+    if (KIND >= 2) {
+      // this unit's sample range: segment rows ky in [ca, ca + nv)
+      const int* rp = t.rowptr + (long long)t.slot_seg[cur.slot] * (t.Nv[0] + 1);
+      const int s0 = rp[cur.ca], s1 = rp[cur.ca + cur.nv];
+      const long long ob = t.ld * (cur.cb + t.n3off) + t.ld * t.N3y * cc;
+      if (KIND == 2) {
+#pragma unroll
+        for (int m = 0; m < F1; ++m) v[m] = (lt < F2) ? st[tswz(lt + F2 * m, li)] : make_float2(0.f, 0.f);
+        __syncthreads();  // the tile becomes the exchange area
+        LN::fwd(v, X, lt, myex, tw);
+        __syncthreads();  // every line's exchange is done
+        if (lt < F1) {
+#pragma unroll
+          for (int k2 = 0; k2 < F2; ++k2) st[tswz(lt + F1 * k2, li)] = X[k2];
+        }
+        __syncthreads();
+        for (int q = s0 + tid; q < s1; q += kThreads) {
+          const int i = t.perm[q];
+          float2 val = cscale(st[tswz(t.kzv[i], t.kyv[i] - cur.ca)], t.scale);
+          if (t.ymeas) val = csub(val, t.ymeas[ob + i]);
+          t.y[ob + i] = val;
+        }
+        cur = nxt;
+        cc = cn;
+        continue;
+      }
+      // KIND 3: the tile from the weighted samples (buffer free once every
+      // earlier store has read it)
+      if (tid == 0) bulk_wait_read0();
+      __syncthreads();
+      for (int e = tid; e < P::TILE / 2; e += kThreads)
+        reinterpret_cast<float4*>(st)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncthreads();
+      const float mb = t.Mb ? t.Mb[cur.cb + t.n3off] : 1.f;
+      for (int q = s0 + tid; q < s1; q += kThreads) {
+        const int i = t.perm[q];
+        const float w = t.We ? mb * t.We[i] : mb;
+        const float2 val = cscale(t.y[ob + i], w);
+        float2* d = &st[tswz(t.kzv[i], t.kyv[i] - cur.ca)];
+        atomicAdd(&d->x, val.x);
+        atomicAdd(&d->y, val.y);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k2 = 0; k2 < F2; ++k2) X[k2] = lt < F1 ? st[tswz(lt + F1 * k2, li)] : make_float2(0.f, 0.f);
+      __syncthreads();  // the tile becomes the exchange area
+      LN::inv(X, v, lt, myex, tw);
+    } else {
 #pragma unroll
     for (int m = 0; m < F1; ++m) v[m] = (lt < F2) ? st[tswz(lt + F2 * m, li)] : make_float2(0.f, 0.f);
     __syncthreads();  // the tile becomes the exchange area
-    float2* myex = st + li * LN::EXSZ;
     LN::fwd(v, X, lt, myex, tw);
     if (lt < F1) {
       if (KIND == 0) {
@@ -228,6 +295,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
     }
     LN::inv(X, v, lt, myex, tw);
+    }
     __syncthreads();  // every line's exchange is done
     if (lt < F2) {
 #pragma unroll
@@ -236,14 +304,14 @@ __global__ void __launch_bounds__(kThreads, 3)
     fence_async_smem();  // the writes above are read by the bulk store
     __syncthreads();
     if (tid == 0) {
-      const int w = KIND == 1 ? cur.slot * C + cc : cur.slot;
+      const int w = KIND >= 1 ? cur.slot * C + cc : cur.slot;
       tma_store_tile(&out_map, cur.ca, t.axis == 2 ? cur.cb : 0, t.axis == 1 ? cur.cb : 0, w, st);
       bulk_commit();
     }
     cur = nxt;
     cc = cn;
   }
-  if (tid == 0) bulk_wait0();
+  if (STORE && tid == 0) bulk_wait0();
 }
 
 // Host side (tmamap.cu): the tensor map of n_vol volumes N0 x N1 x N2
@@ -256,7 +324,7 @@ template <int F1, int F2>
 struct TmaLaunch {
   using P = TPipe<F1, F2>;
   struct Occ {
-    int per_sm[2] = {0, 0}, sms = 0;
+    int per_sm[4] = {0, 0, 0, 0}, sms = 0;
   };
   template <int KIND>
   static void prep(Occ& o) {
@@ -267,6 +335,8 @@ struct TmaLaunch {
     Occ o;
     prep<0>(o);
     prep<1>(o);
+    prep<2>(o);
+    prep<3>(o);
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev);
@@ -277,15 +347,17 @@ struct TmaLaunch {
     static const Occ occ = init();
     if (occ.per_sm[kind] <= 0 || occ.sms <= 0) return false;
     const long long tiles = (long long)((t.Nv[0] + 15) / 16) * t.Nv[t.axis == 1 ? 2 : 1];
-    const int S = kind == 1 ? t.n_slots : t.n_vol, C = kind == 1 ? t.C : 1;
+    const int S = kind >= 1 ? t.n_slots : t.n_vol, C = kind >= 1 ? t.C : 1;
     const long long units = tiles * S;
     if (units == 0 || units * C >= (1LL << 31)) return false;
     const long long cap = (long long)occ.sms * occ.per_sm[kind];
     const unsigned grid = (unsigned)(units < cap ? units : cap);
-    if (kind == 0)
-      tma_kernel<F1, F2, 0><<<grid, kThreads, P::SMEM, s>>>(in, out, t, tw, (int)tiles, shared_input);
-    else
-      tma_kernel<F1, F2, 1><<<grid, kThreads, P::SMEM, s>>>(in, out, t, tw, (int)tiles, shared_input);
+    switch (kind) {
+      case 0: tma_kernel<F1, F2, 0><<<grid, kThreads, P::SMEM, s>>>(in, out, t, tw, (int)tiles, shared_input); break;
+      case 1: tma_kernel<F1, F2, 1><<<grid, kThreads, P::SMEM, s>>>(in, out, t, tw, (int)tiles, shared_input); break;
+      case 2: tma_kernel<F1, F2, 2><<<grid, kThreads, P::SMEM, s>>>(in, out, t, tw, (int)tiles, shared_input); break;
+      default: tma_kernel<F1, F2, 3><<<grid, kThreads, P::SMEM, s>>>(in, out, t, tw, (int)tiles, shared_input); break;
+    }
     return true;
   }
 };

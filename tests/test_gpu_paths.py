@@ -1,4 +1,5 @@
-"""The kernel variants of one operation agree: the TMA tile-copy passes, the
+"""The kernel variants of one operation agree: the TMA tile-copy passes (and
+the TMA gather / scatter of encode and decode), the
 cp.async-pipelined passes (DISORDER_NO_TMA=1) and the one-tile-per-CTA
 kernels (DISORDER_NO_PIPE=1) compute the same arithmetic with different data
 movement, so the sinc rigid transform and the normal operator must match to
@@ -39,8 +40,11 @@ ky, kz, nEc, mSt, _ = synth.sample_lists(H, S)
 E = db.Struct(Tr=T, NMs=S, NSe=S + 1, Sf=ctx.upload(Sf), grids=g, ky=ky, kz=kz, nEc=nEc, mSt=mSt)
 we = rng.uniform(0.5, 1.5, int(nEc[-1])).astype(np.float32)
 ed = db.encodedecode(x, E, db.Struct(We=we), ctx=ctx)
+yy = db.encode(x, E, ctx=ctx)
+mb = rng.uniform(0.0, 1.0, N[2]).astype(np.float32)
+dd = db.decode(yy, db.Struct(We=we, Mb=mb), E, ctx=ctx)
 ctx.synchronize()
-np.savez(out, fw=fw, inv=inv, ed=ed)
+np.savez(out, fw=fw, inv=inv, ed=ed, y=yy, dec=dd)
 """
 
 
@@ -62,7 +66,7 @@ def test_tma_pipe_and_tile_kernels_agree(tmp_path):
     tma = _run(tmp_path, "tma", {})
     pipe = _run(tmp_path, "pipe", {"DISORDER_NO_TMA": "1"})
     tile = _run(tmp_path, "tile", {"DISORDER_NO_PIPE": "1"})
-    for k in ("fw", "inv", "ed"):
+    for k in ("fw", "inv", "ed", "y", "dec"):
         assert _rel(tma[k], pipe[k]) < 1e-6, k
         # the one-tile kernels read full phase tables (single-precision grid
         # products) where the pipelined ones use per-row seeds
