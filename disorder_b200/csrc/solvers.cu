@@ -202,7 +202,21 @@ int dis_weighted_norm(disorder_ctx_s* ctx, const float2* b, const float* w, long
 // ---------------------------------------------------------------- energy
 // computeEnergy (Reconstruction/computeEnergy.m:34-80) for no=2.
 int dis_energy(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* y, const float2* x, const float2* Sf,
-               int C, const float* T, const float* rowW, const float* R_Ti, float2* rbuf, double* En) {
+               int C, const float* T, const float* rowW, const float* R_Ti, float2* rbuf, double* En, int n3_lo,
+               int n3_cnt) {
+  // readout rows outside [n3_lo, n3_lo + n3_cnt) have zero weight: their
+  // samples are neither encoded nor summed (n3_cnt < 0: all rows)
+  if (n3_cnt < 0 || !rowW) {
+    n3_lo = 0;
+    n3_cnt = plan->N[2];
+  }
+  double reg = 0;
+  if (R_Ti) DIS_TRY(dis_ti_energy(ctx, x, R_Ti, plan->V, &reg));
+  En[1] = reg;
+  if (n3_cnt == 0) {
+    En[0] = 0;
+    return DISORDER_OK;
+  }
   EncodeSpec sp;
   sp.x = x;
   sp.Sf = Sf;
@@ -210,10 +224,10 @@ int dis_energy(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* y
   sp.T = T;
   sp.T_n = plan->n_mot;
   for (int s = 0; s < plan->n_seg; ++s) sp.segs.push_back(s);
-  sp.n3_lo = 0;
-  sp.N3c = plan->N[2];
+  sp.n3_lo = n3_lo;
+  sp.N3c = n3_cnt;
   sp.y_ld = plan->n_samples;
-  sp.y_n3off = 0;
+  sp.y_n3off = n3_lo;
   sp.y_N3 = plan->N[2];
   DIS_TRY(dis_encode_segments(ctx, plan, sp, rbuf, y));
   // sum |r|^2 * rowW[n3] over all samples
@@ -234,17 +248,14 @@ int dis_energy(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* y
     DIS_TRY(dis_upload_ints(ctx, &ws, all, &d_all));
     double* d_out = ws.take<double>((size_t)plan->n_seg * 28);
     if (!d_out) return dis_set_error(ctx, DISORDER_OOM, "energy workspace");
-    DIS_TRY(dis_seg_sums(ctx, plan, d_all, plan->n_seg, rbuf, nullptr, 0, plan->n_samples, 0, plan->N[2],
+    DIS_TRY(dis_seg_sums(ctx, plan, d_all, plan->n_seg, rbuf, nullptr, 0, plan->n_samples, n3_lo, n3_cnt,
                          plan->N[2], C, rowW, d_out, &ws));
     std::vector<double> h((size_t)plan->n_seg * 28);
     DIS_CUDA_TRY(cudaMemcpyAsync(h.data(), d_out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     for (int s = 0; s < plan->n_seg; ++s) fid += h[(size_t)s * 28];
   }
-  double reg = 0;
-  if (R_Ti) DIS_TRY(dis_ti_energy(ctx, x, R_Ti, plan->V, &reg));
   En[0] = fid;
-  En[1] = reg;
   return DISORDER_OK;
 }
 
@@ -297,9 +308,23 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
     return dis_set_error(ctx, DISORDER_OOM, "CG workspace");
   DIS_TRY(dis_build_weight_map(ctx, plan, s.We, wmap, 1.f));
   const bool haveRow = s.Mb || s.Mbe;
+  int e_lo = 0, e_cnt = -1;  // readout rows with nonzero energy weight
   if (haveRow) {
     rowweight_kernel<<<1, 256, 0, ctx->stream>>>(s.Mb, s.Mbe, plan->N[2], roww);
     dis_count(ctx);
+    if (tolType == 6) {
+      std::vector<float> hw(plan->N[2]);
+      DIS_CUDA_TRY(cudaMemcpyAsync(hw.data(), roww, hw.size() * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+      DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      int lo = plan->N[2], hi = -1;
+      for (int k = 0; k < plan->N[2]; ++k)
+        if (hw[k] != 0.f) {
+          lo = std::min(lo, k);
+          hi = k;
+        }
+      e_lo = hi < 0 ? 0 : lo;
+      e_cnt = hi < 0 ? 0 : hi - lo + 1;
+    }
   }
   Workspace rws;
   DIS_TRY(dis_small(ctx, &rws));
@@ -381,7 +406,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
     DIS_TRY(red_finish(R, &rn_re, &rn_im));
     if (n % NitTest == 1 && tolType == 6) {
       double e2[2];
-      DIS_TRY(dis_energy(ctx, plan, s.y, x, s.Sf, s.C, s.T, haveRow ? roww : nullptr, s.R_Ti, rbuf, e2));
+      DIS_TRY(dis_energy(ctx, plan, s.y, x, s.Sf, s.C, s.T, haveRow ? roww : nullptr, s.R_Ti, rbuf, e2, e_lo, e_cnt));
       Ecol.push_back(e2[0]);
       Ecol.push_back(e2[1]);
     }

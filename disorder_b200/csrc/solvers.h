@@ -30,6 +30,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
 int dis_lm_step(disorder_ctx_s* ctx, const disorder_plan_s* plan, const LMSpec& s, float* T, float* w, uint8_t* cT,
                 double* En, double* EnPrev);
 int dis_energy(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* y, const float2* x, const float2* Sf,
-               int C, const float* T, const float* rowW, const float* R_Ti, float2* rbuf, double* En);
+               int C, const float* T, const float* rowW, const float* R_Ti, float2* rbuf, double* En, int n3_lo = 0,
+               int n3_cnt = -1);
 int dis_ti_energy(disorder_ctx_s* ctx, const float2* x, const float* ti, long long n, double* out);
 int dis_weighted_norm(disorder_ctx_s* ctx, const float2* b, const float* w, long long n, double* out);
