@@ -534,10 +534,14 @@ def main():
     ctx.event(2)
     Sd = ctx.upload(Sh)
     yd = ctx.upload(yh)
+    ctx.event(6)
     xe, _, _ = one(Sd, yd)
+    ctx.event(7)
     xh = xe.numpy()
     ctx.event(3)
     e2e_ms = ctx.elapsed_ms(2, 3)
+    e2e_parts = {"upload_s": ctx.elapsed_ms(2, 6) * 1e-3, "recon_s": ctx.elapsed_ms(6, 7) * 1e-3,
+                 "download_s": ctx.elapsed_ms(7, 3) * 1e-3}
     del Sd, yd, xh
 
     # roofline of the dominant kernel family: the line passes of the sinc rigid
@@ -585,7 +589,7 @@ def main():
            "schedule": counts, "phases_s": {k: round(v, 4) for k, v in phases.items()},
            "gpu_launches": int(launches / args.steps), "clocks": clocks,
            "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": int(Sh.nbytes + yh.nbytes),
-                   "d2h_bytes_per_step": int(V * 8)},
+                   "d2h_bytes_per_step": int(V * 8), "parts": {k: round(v, 4) for k, v in e2e_parts.items()}},
            "roofline": roof}
     if rank == 0 and not args.no_cpu:
         est, thr, desc = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], counts)
