@@ -38,9 +38,9 @@ SMALL = dict(N=(64, 64, 48), coils=8, coils_kept=6, shots=16, rot_deg=5.0, trans
              ellipsoids=12, seed=2001)
 NOMINAL_COUNTS = {"outer": [20, 20], "cg_final": 30}  # nominal schedule for the CPU reference estimate
 # DRAM bytes (read + write) per line-pass launch at 64 states: an ncu capture of
-# the strided and contiguous passes at 4 states (679.5 MB per launch, mean of
-# launches 2-4 of a forward transform) scaled by 16; stores still held in L2
-# when a launch ends are not counted.
+# the contiguous (pipe_kernel) and strided (tma_kernel) passes at 4 states
+# (679.5 MB per launch, launches 2-4 of a forward transform) scaled by 16;
+# stores still held in L2 when a launch ends are not counted.
 TRAFFIC_PER_LAUNCH = 10.87e9
 
 
@@ -577,7 +577,8 @@ def main():
     achieved = bytes_per_launch / (t_fwd / n_pass * 1e-3) / 1e9
     peak, pkind = peaks()
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": TRAFFIC_PER_LAUNCH, "kernel": "fp::pipe_kernel (pipelined sinc-transform line pass)",
+            "traffic": TRAFFIC_PER_LAUNCH,
+            "kernel": "fp::pipe_kernel (dim-1 passes) + fp::tma_kernel (dim-2/3 passes): sinc-transform line passes",
             "peak_kind": pkind, "bytes_per_launch": bytes_per_launch,
             "timing": "one forward transform (11 launches, phase-seed build included) through the C ABI, "
                       "%d states, CUDA events, mean of %d" % (S, reps)}
