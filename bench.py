@@ -408,6 +408,17 @@ def operator_only(cfg, S, warmup, steps, profile_region=False):
                       "results": res}))
 
 
+def phase_split(log):
+    """Host-side phase durations of one reconstruction (the solver calls
+    synchronise, so these include their GPU time)."""
+    phases, prev = {}, 0.0
+    for e in log.events:
+        key = e["step"] + ("_L%d" % e["level"] if "level" in e else "")
+        phases[key] = phases.get(key, 0.0) + (e["t"] - prev)
+        prev = e["t"]
+    return phases
+
+
 # ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -506,13 +517,7 @@ def main():
         ms = float(t.item())
     err = nrmse(ctx, x, sc.x_gt_host)
     motion_err = float(np.max(np.abs(T - sc.T_gt)[:, :3])), float(np.degrees(np.max(np.abs(T - sc.T_gt)[:, 3:])))
-    # host-side phase durations of the last timed reconstruction (the solver
-    # calls synchronise, so these include their GPU time)
-    phases, prev = {}, 0.0
-    for e in logs[-1].events:
-        key = e["step"] + ("_L%d" % e["level"] if "level" in e else "")
-        phases[key] = phases.get(key, 0.0) + (e["t"] - prev)
-        prev = e["t"]
+    phases = phase_split(logs[-1])
     counts = {"outer": [sum(1 for e in logs[-1].events if e["step"] == "lm" and e["level"] == lv) for lv in (0, 1)],
               "cg_final": sum(e["iters"] for e in logs[-1].events if e["step"] == "cg" and e["level"] == 2)}
 
@@ -531,17 +536,21 @@ def main():
     yh, _ybuf = pinned(sc.y)
     ctx.synchronize()
     t0 = time.perf_counter()
+    eclk = NvmlClockSampler(local)
+    eclk.start()
     ctx.event(2)
     Sd = ctx.upload(Sh)
     yd = ctx.upload(yh)
     ctx.event(6)
-    xe, _, _ = one(Sd, yd)
+    xe, _, elog = one(Sd, yd)
     ctx.event(7)
     xh = xe.numpy()
     ctx.event(3)
     e2e_ms = ctx.elapsed_ms(2, 3)
     e2e_parts = {"upload_s": ctx.elapsed_ms(2, 6) * 1e-3, "recon_s": ctx.elapsed_ms(6, 7) * 1e-3,
                  "download_s": ctx.elapsed_ms(7, 3) * 1e-3}
+    e2e_phases = phase_split(elog)
+    e2e_clocks = eclk.stop()
     del Sd, yd, xh
 
     # roofline of the dominant kernel family: the line passes of the sinc rigid
@@ -590,7 +599,8 @@ def main():
            "schedule": counts, "phases_s": {k: round(v, 4) for k, v in phases.items()},
            "gpu_launches": int(launches / args.steps), "clocks": clocks,
            "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": int(Sh.nbytes + yh.nbytes),
-                   "d2h_bytes_per_step": int(V * 8), "parts": {k: round(v, 4) for k, v in e2e_parts.items()}},
+                   "d2h_bytes_per_step": int(V * 8), "parts": {k: round(v, 4) for k, v in e2e_parts.items()},
+                   "phases_s": {k: round(v, 4) for k, v in e2e_phases.items()}, "clocks": e2e_clocks},
            "roofline": roof}
     if rank == 0 and not args.no_cpu:
         est, thr, desc = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], counts)

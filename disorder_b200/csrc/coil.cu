@@ -5,6 +5,8 @@
 // reference (Fs{1}, Fs{2}: rows of build1DFTM(N,1)) are evaluated as a full
 // FFT along dim 1 followed by an FFT along dim 2 and a gather of each
 // segment's samples, which is the same linear map.
+#include <cmath>
+
 #include "fastpass.h"
 #include "internal.h"
 
@@ -360,15 +362,19 @@ int dis_coil_scatter_ifft2(disorder_ctx_s* ctx, const disorder_plan_s* plan, con
 }
 
 int dis_coil_fft2_weight(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, float2* A,
-                         const float* wmap) {
+                         const float* wmap, float2* ys, long long ys_ld, int ys_n3off, int ys_N3) {
   if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
   // the fast kernels apply w and the explicit inverse; the 1/(N1*N2) of the
   // inverse DFTs is applied by the combine step
-  if (dis_use_fast() && dis_use_pipe() && dis_fast_tma_weight(ctx, a, A, wmap, plan->d_tw[1])) {
+  const float enc_scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
+  if (dis_use_fast() && dis_use_pipe() &&
+      dis_fast_tma_weight(ctx, a, A, wmap, plan->d_tw[1], plan, ys, ys_ld, ys_n3off, ys_N3, enc_scale)) {
     dis_count(ctx);
     DIS_CUDA_TRY(cudaGetLastError());
     return DISORDER_OK;
   }
+  // the forward samples from a separate gather when the fused pass does not apply
+  if (ys) DIS_TRY(dis_coil_fft2_gather(ctx, plan, a, A, ys, ys_ld, ys_n3off, ys_N3, nullptr, enc_scale));
   if (dis_use_fast() && dis_use_pipe() && dis_fast_wpipe(a.N2, a, A, wmap, plan->d_tw[1], ctx->stream)) {
     dis_count(ctx);
     DIS_CUDA_TRY(cudaGetLastError());

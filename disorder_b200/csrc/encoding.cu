@@ -340,6 +340,7 @@ int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, 
   const int N3 = plan->N[2];
   bool first = true;
   if (dis_plane_usable(plan, sp.C, sp.segs)) {
+    if (sp.ys) return dis_set_error(ctx, DISORDER_BAD_ARG, "encodedecode: sample output needs the three-pass path");
     const int ch = plane_chunk(plan, nsg, V * sizeof(float2));
     Workspace ws;
     DIS_TRY(dis_workspace(ctx, (size_t)ch * V * sizeof(float2) + 2 * dis_table_bytes(plan, ch, false) + (1 << 20),
@@ -402,7 +403,7 @@ int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, 
     }
     CoilArgs ca = coil_args(plan, sp.Sf, sp.C, 0, N3, Vz, n, d_seg);
     DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, z, A));
-    DIS_TRY(dis_coil_fft2_weight(ctx, plan, ca, A, sp.wmap));
+    DIS_TRY(dis_coil_fft2_weight(ctx, plan, ca, A, sp.wmap, sp.ys, plan->n_samples, 0, N3));
     ca.Vz = V;
     const float scale = (float)(1.0 / ((double)plan->N[0] * plan->N[1]));
     DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));

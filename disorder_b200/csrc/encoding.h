@@ -36,6 +36,9 @@ struct EncodeDecodeSpec {
   std::vector<int> segs;
   const float* wmap = nullptr;  // [seg][N1][N2] (kz fastest) sample weights of each grid point (three-pass path)
   const float* We = nullptr;    // per-sample weights (plane path), NULL for 1
+  // when set (three-pass path only), the samples of the forward half, E x in
+  // encode's layout (y_ld = n_samples, all readout rows), are written here
+  float2* ys = nullptr;
 };
 
 size_t dis_budget_bytes();

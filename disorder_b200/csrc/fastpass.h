@@ -16,7 +16,11 @@ bool dis_fast_wpipe(int n, const CoilArgs& a, float2* A, const float* wmap, cons
 // TMA tile-copy variants (tmapass.cuh) of the strided transform passes and
 // of the weighted pass; false when the pass does not fit them.
 bool dis_fast_tma_line(disorder_ctx_s* ctx, const LinePassArgs& a);
-bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, const float* wmap, const float2* tw);
+// With ys non-null the weighted pass also writes the forward samples (encode's
+// layout and scale) into ys.
+bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, const float* wmap, const float2* tw,
+                         const disorder_plan_s* plan = nullptr, float2* ys = nullptr, long long ld = 0, int n3off = 0,
+                         int N3y = 0, float scale = 1.f);
 bool dis_fast_tma_gather(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* A,
                          float2* y, long long y_ld, int y_n3off, int y_N3, const float2* y_meas, float scale);
 bool dis_fast_tma_scatter(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* y,

@@ -193,7 +193,8 @@ int dis_coil_scatter_ifft2(disorder_ctx_s* ctx, const disorder_plan_s* plan, con
                            const float2* y, long long y_ld, int y_n3off, int y_N3, const float* We,
                            const float* Mb, float2* A);
 int dis_coil_fft2_weight(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, float2* A,
-                         const float* wmap /*[seg][N1][N2], kz fastest*/);
+                         const float* wmap /*[seg][N1][N2], kz fastest*/,
+                         float2* ys = nullptr, long long ys_ld = 0, int ys_n3off = 0, int ys_N3 = 0);
 int dis_coil_ifft1_combine(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a,
                            const float2* A, float2* u, float scale);
 int dis_build_weight_map(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float* We, float* wmap,

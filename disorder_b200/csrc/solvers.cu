@@ -130,6 +130,20 @@ __global__ void init_kernel(const float2* __restrict__ b, const float2* __restri
 }
 
 // p = z + d p
+// r = -y (the residual of x = 0)
+__global__ void neg_kernel(float2* __restrict__ r, const float2* __restrict__ y, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 v = y[i];
+    r[i] = make_float2(-v.x, -v.y);
+  }
+}
+
+// r += g e (the sample residual follows x += g p with e = E p)
+__global__ void caxpy_kernel(float2* __restrict__ r, const float2* __restrict__ e, float2 g, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    r[i] = cadd(r[i], cmul(g, e[i]));
+}
+
 __global__ void pupdate_kernel(float2* __restrict__ p, const float2* __restrict__ z, float2 d, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     p[i] = cadd(z[i], cmul(d, p[i]));
@@ -230,6 +244,22 @@ int dis_energy(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* y
   sp.y_n3off = n3_lo;
   sp.y_N3 = plan->N[2];
   DIS_TRY(dis_encode_segments(ctx, plan, sp, rbuf, y));
+  return dis_fidelity(ctx, plan, rbuf, C, rowW, En, n3_lo, n3_cnt);
+}
+
+// En[0] = sum over the samples of rows [n3_lo, n3_lo + n3_cnt) of rowW[n3] |r|^2
+// (all rows and weight 1 without rowW), for a residual r = E x - y in
+// encode's layout.
+int dis_fidelity(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* rbuf, int C, const float* rowW,
+                 double* En, int n3_lo, int n3_cnt) {
+  if (n3_cnt < 0 || !rowW) {
+    n3_lo = 0;
+    n3_cnt = plan->N[2];
+  }
+  if (n3_cnt == 0) {
+    En[0] = 0;
+    return DISORDER_OK;
+  }
   // sum |r|^2 * rowW[n3] over all samples
   const long long n = plan->n_samples * plan->N[2] * (long long)C;
   Workspace ws;
@@ -293,7 +323,16 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   // persistent solver vectors: b, r, z, p, ehe + wmap + residual buffer + row weights
   const long long wm = (long long)plan->n_seg * plan->N[0] * plan->N[1];
   const long long ny = plan->n_samples * plan->N[2] * (long long)s.C;
-  const size_t need = sizeof(float2) * (5 * V + (tolType == 6 ? ny : 0)) + sizeof(float) * (wm + plan->N[2]) + (1 << 20);
+  // With the Energy tolerance the residual r = E x - y is kept in sample
+  // space: each normal operator on p also writes E p (ebuf), r += g E p
+  // follows x += g p, and the energy is a reduction of r, the same quantity
+  // the reference gets from an encode of x (computeEnergy.m:52-70). The
+  // plane path does not produce E p: it encodes x at each evaluation.
+  std::vector<int> all_segs;
+  for (int q = 0; q < plan->n_seg; ++q) all_segs.push_back(q);
+  const bool track = tolType == 6 && !dis_plane_usable(plan, s.C, all_segs);
+  const size_t need = sizeof(float2) * (5 * V + (tolType == 6 ? ny : 0) + (track ? ny : 0)) +
+                      sizeof(float) * (wm + plan->N[2]) + (1 << 20);
   Workspace ws;
   DIS_TRY(dis_workspace2(ctx, need, &ws));
   float2* b = ws.take<float2>(V);
@@ -304,7 +343,8 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   float* wmap = ws.take<float>(wm);
   float* roww = ws.take<float>(plan->N[2]);
   float2* rbuf = tolType == 6 ? ws.take<float2>(ny) : nullptr;
-  if (!b || !r || !z || !p || !ehe || !wmap || !roww || (tolType == 6 && !rbuf))
+  float2* ebuf = track ? ws.take<float2>(ny) : nullptr;
+  if (!b || !r || !z || !p || !ehe || !wmap || !roww || (tolType == 6 && !rbuf) || (track && !ebuf))
     return dis_set_error(ctx, DISORDER_OOM, "CG workspace");
   DIS_TRY(dis_build_weight_map(ctx, plan, s.We, wmap, 1.f));
   const bool haveRow = s.Mb || s.Mbe;
@@ -357,14 +397,15 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   es.segs = segs;
   es.wmap = wmap;
   es.We = s.We;
-  auto normal_op = [&](const float2* in, float2* out) -> int {
+  auto normal_op = [&](const float2* in, float2* out, float2* samples) -> int {
     es.x = in;
+    es.ys = samples;
     return dis_encodedecode_segments(ctx, plan, es, out);
   };
   double dummy = 0;
   // EHE for the initial guess (:53-56)
   if (x_init) {
-    DIS_TRY(normal_op(x, ehe));
+    DIS_TRY(normal_op(x, ehe, nullptr));
     pap_kernel<<<blocks, 256, 0, ctx->stream>>>(x, ehe, s.C_Ma, s.R_Ti, V, R.part);
     dis_count(ctx);
     DIS_TRY(red_finish(R, &dummy, nullptr));
@@ -384,11 +425,32 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   *n_en = 0;
   *nn = 0;
   if (std::hypot(rs_re, rs_im) < 1e-6) return DISORDER_OK;  // :70-75
+  if (track) {
+    // r = E x0 - y (x0 = 0: r = -y)
+    if (x_init) {
+      EncodeSpec sp;
+      sp.x = x;
+      sp.Sf = s.Sf;
+      sp.C = s.C;
+      sp.T = s.T;
+      sp.T_n = plan->n_mot;
+      sp.segs = all_segs;
+      sp.n3_lo = 0;
+      sp.N3c = plan->N[2];
+      sp.y_ld = plan->n_samples;
+      sp.y_n3off = 0;
+      sp.y_N3 = plan->N[2];
+      DIS_TRY(dis_encode_segments(ctx, plan, sp, rbuf, s.y));
+    } else {
+      neg_kernel<<<blocks, 256, 0, ctx->stream>>>(rbuf, s.y, ny);
+      dis_count(ctx);
+    }
+  }
   double err = INFINITY;
   std::vector<double> Ecol;  // energies of odd iterations, 2 per column
   int n = 0;
   for (n = 1; n <= nIt; ++n) {
-    DIS_TRY(normal_op(p, ehe));  // :80
+    DIS_TRY(normal_op(p, ehe, ebuf));  // :80 (and E p for the residual)
     pap_kernel<<<blocks, 256, 0, ctx->stream>>>(p, ehe, s.C_Ma, s.R_Ti, V, R.part);
     dis_count(ctx);
     double pa_re = 0, pa_im = 0;
@@ -404,9 +466,20 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
     dis_count(ctx);
     double rn_re = 0, rn_im = 0;
     DIS_TRY(red_finish(R, &rn_re, &rn_im));
+    if (track) {
+      caxpy_kernel<<<blocks, 256, 0, ctx->stream>>>(rbuf, ebuf, make_float2((float)g_re, (float)g_im), ny);
+      dis_count(ctx);
+    }
     if (n % NitTest == 1 && tolType == 6) {
       double e2[2];
-      DIS_TRY(dis_energy(ctx, plan, s.y, x, s.Sf, s.C, s.T, haveRow ? roww : nullptr, s.R_Ti, rbuf, e2, e_lo, e_cnt));
+      if (track) {
+        DIS_TRY(dis_fidelity(ctx, plan, rbuf, s.C, haveRow ? roww : nullptr, e2, e_lo, e_cnt));
+        e2[1] = 0;
+        if (s.R_Ti) DIS_TRY(dis_ti_energy(ctx, x, s.R_Ti, V, &e2[1]));
+      } else {
+        DIS_TRY(dis_energy(ctx, plan, s.y, x, s.Sf, s.C, s.T, haveRow ? roww : nullptr, s.R_Ti, rbuf, e2, e_lo,
+                           e_cnt));
+      }
       Ecol.push_back(e2[0]);
       Ecol.push_back(e2[1]);
     }

@@ -32,5 +32,9 @@ int dis_lm_step(disorder_ctx_s* ctx, const disorder_plan_s* plan, const LMSpec& 
 int dis_energy(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* y, const float2* x, const float2* Sf,
                int C, const float* T, const float* rowW, const float* R_Ti, float2* rbuf, double* En, int n3_lo = 0,
                int n3_cnt = -1);
+// fidelity of a residual r = E x - y (encode's layout): sum of rowW[n3] |r|^2
+// over rows [n3_lo, n3_lo + n3_cnt) (n3_cnt < 0 or no rowW: all rows, weight 1)
+int dis_fidelity(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* rbuf, int C, const float* rowW,
+                 double* En, int n3_lo = 0, int n3_cnt = -1);
 int dis_ti_energy(disorder_ctx_s* ctx, const float2* x, const float* ti, long long n, double* out);
 int dis_weighted_norm(disorder_ctx_s* ctx, const float2* b, const float* w, long long n, double* out);

@@ -107,7 +107,8 @@ bool dis_fast_tma_line(disorder_ctx_s* ctx, const LinePassArgs& a) {
   return launch_size(n, 0, in, out, t, a.tw, shared_input, ctx->stream);
 }
 
-bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, const float* wmap, const float2* tw) {
+bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, const float* wmap, const float2* tw,
+                         const disorder_plan_s* plan, float2* ys, long long ld, int n3off, int N3y, float scale) {
   if (!tma_enabled() || !ctx->d_err || !has_tma_size(a.N2)) return false;
   const int Nv[3] = {a.N1, a.N2, a.N3c};
   const long long Vc = (long long)a.N1 * a.N2 * a.N3c;
@@ -115,7 +116,7 @@ bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, cons
   if (nvol < 1 || nvol >= (1LL << 31)) return false;
   CUtensorMap m;
   if (!dis_tmap_volumes(&m, A, Nv, 1, Vc, (int)nvol)) return false;
-  fp::TArgs t;
+  fp::TArgs t = fp::TArgs();
   for (int i = 0; i < 3; ++i) t.Nv[i] = Nv[i];
   t.axis = 1;
   t.n_vol = (int)nvol;
@@ -124,6 +125,17 @@ bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, cons
   t.slot_seg = a.d_slot_seg;
   t.wmap = wmap;
   t.err = ctx->d_err;
+  if (ys) {
+    t.y = ys;
+    t.ld = ld;
+    t.n3off = n3off;
+    t.N3y = N3y;
+    t.scale = scale;
+    t.rowptr = plan->d_rowptr;
+    t.perm = plan->d_perm;
+    t.kyv = plan->d_ky;
+    t.kzv = plan->d_kz;
+  }
   return launch_size(a.N2, 1, m, m, t, tw, 0, ctx->stream);
 }
 

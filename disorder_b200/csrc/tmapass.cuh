@@ -84,7 +84,9 @@ struct TPipe {
 
 // KIND 0: transform pass (coefficient from the line's phase seeds, a.Sd);
 // KIND 1: normal-operator weighting (coefficient = sample weight, volumes are
-// the per-coil intermediates, unit = (tile, slot) walking its C coils);
+// the per-coil intermediates, unit = (tile, slot) walking its C coils); with
+// t.y set it also writes the tile's samples of the forward DFT (what encode
+// would produce for the same input) before weighting them;
 // KIND 2: encode gather (DFT along dim 2, then the segment's samples of the
 // tile's ky rows are read out of the tile into y; no store);
 // KIND 3: decode scatter (the tile is built from the weighted samples, then
@@ -271,6 +273,22 @@ __global__ void __launch_bounds__(kThreads, 3)
     for (int m = 0; m < F1; ++m) v[m] = (lt < F2) ? st[tswz(lt + F2 * m, li)] : make_float2(0.f, 0.f);
     __syncthreads();  // the tile becomes the exchange area
     LN::fwd(v, X, lt, myex, tw);
+    if (KIND == 1 && t.y) {
+      // the segment's samples of this tile, as encode's gather writes them
+      __syncthreads();  // every line's exchange is done
+      if (lt < F1) {
+#pragma unroll
+        for (int k2 = 0; k2 < F2; ++k2) st[tswz(lt + F1 * k2, li)] = X[k2];
+      }
+      __syncthreads();
+      const int* rp = t.rowptr + (long long)t.slot_seg[cur.slot] * (t.Nv[0] + 1);
+      const long long ob = t.ld * (cur.cb + t.n3off) + t.ld * t.N3y * cc;
+      for (int q = rp[cur.ca] + tid; q < rp[cur.ca + cur.nv]; q += kThreads) {
+        const int i = t.perm[q];
+        t.y[ob + i] = cscale(st[tswz(t.kzv[i], t.kyv[i] - cur.ca)], t.scale);
+      }
+      __syncthreads();  // the tile is the exchange area again
+    }
     if (lt < F1) {
       if (KIND == 0) {
         constexpr int KP = F2 / 2;

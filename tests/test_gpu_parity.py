@@ -217,12 +217,14 @@ def test_compute_energy(ctx):
     assert abs(En[1] - Eno[1]) / Eno[1] < TOL
 
 
-@pytest.mark.parametrize("tolType,nIt", [("RelativeResidual2Error", 4), ("Energy", 7)])
-def test_cg(ctx, tolType, nIt):
+# (44, 44, 22) reaches the TMA weighted pass, which also emits the forward
+# samples that CG's Energy tolerance tracks; (16, 16, 12) the separate gather
+@pytest.mark.parametrize("tolType,nIt,N", [("RelativeResidual2Error", 4, (16, 16, 12)), ("Energy", 7, (16, 16, 12)),
+                                          ("Energy", 7, (44, 44, 22))])
+def test_cg(ctx, tolType, nIt, N):
     import disorder_b200 as db
     from oracle import encoding as oenc
     from oracle import solvers as osol
-    N = (16, 16, 12)
     Ed, Eo, sc = _E_pair(ctx, N, 4, 4, seed=31)
     y = oenc.encode(sc.x_gt.astype(np.complex128), Eo)
     Se = (1.0 / (np.sum(np.abs(sc.S) ** 2, axis=3) + 1e-9)).astype(np.float32)
