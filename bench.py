@@ -419,6 +419,27 @@ def phase_split(log):
     return phases
 
 
+# ---------------------------------------------------------------- ranks
+def replica_seed(seed, rank):
+    """Each replica reconstructs its own scan: the synthetic seed moves with the rank."""
+    return seed + 97 * rank
+
+
+def ranks_max(value, device):
+    """Max of a per-rank timing over the process group (every rank calls it)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
 # ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -474,21 +495,16 @@ def main():
     from disorder_b200 import recon
     ctx = db.Context(local)
     cfg_r = dict(cfg)
-    cfg_r["seed"] = cfg["seed"] + 97 * rank
+    cfg_r["seed"] = replica_seed(cfg["seed"], rank)
     sc = build_scan(ctx, cfg_r, use_torch=True)
 
     def one(S, y):
         return recon.aligned_reconstruction(ctx, S, y, sc.H, cfg["shots"], cfg["N"], perc=cfg["coils_kept"])
 
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
     for _ in range(args.warmup):
         x, T, log = one(sc.S, sc.y)
     ctx.synchronize()
-    barrier()
+    barrier(world)
     clk = NvmlClockSampler(local)
     clk.start()
     l0 = ctx.launches
@@ -507,14 +523,10 @@ def main():
     ms_total = ctx.elapsed_ms(0, 1)
     launches = ctx.launches - l0
     clocks = clk.stop()
-    barrier()
+    barrier(world)
     ms = ms_total / args.steps
     if world > 1:
-        import torch
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda:%d" % local)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = ranks_max(ms, "cuda:%d" % local)
     err = nrmse(ctx, x, sc.x_gt_host)
     motion_err = float(np.max(np.abs(T - sc.T_gt)[:, :3])), float(np.degrees(np.max(np.abs(T - sc.T_gt)[:, 3:])))
     phases = phase_split(logs[-1])
