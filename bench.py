@@ -419,6 +419,37 @@ def phase_split(log):
     return phases
 
 
+def learned_arm(ctx, sc, cfg, one_plain_s, counts=None):
+    """One reconstruction with the learned proposal (after one untimed warm-up
+    run): seconds, NRMSE, motion error, outer iterations, proposals kept and
+    LM state-steps, beside the plain method's."""
+    from disorder_b200 import proposal, recon
+    if not os.path.exists(proposal.WEIGHTS):
+        return {"unavailable": "no trained proposal weights at %s" % os.path.relpath(proposal.WEIGHTS, ROOT)}
+    net = proposal.MotionNet.load(ctx, proposal.WEIGHTS)
+
+    def run():
+        return recon.aligned_reconstruction(ctx, sc.S, sc.y, sc.H, cfg["shots"], cfg["N"], perc=cfg["coils_kept"],
+                                            proposal=net)
+
+    run()
+    ctx.synchronize()
+    ctx.event(10)
+    x, T, log = run()
+    ctx.event(11)
+    t = ctx.elapsed_ms(10, 11) * 1e-3
+    ev = log.events
+    d = np.asarray(T, float) - np.asarray(sc.T_gt, float)
+    return {"value": t, "unit": "s", "vs_plain": t / one_plain_s, "nrmse": nrmse(ctx, x, sc.x_gt_host),
+            "motion_max_err": {"trans_vox": float(np.max(np.abs(d[:, :3]))),
+                               "rot_deg": float(np.degrees(np.max(np.abs(d[:, 3:]))))},
+            "outer": [sum(1 for e in ev if e["step"] == "lm" and e["level"] == lv) for lv in (0, 1)],
+            "proposals_kept": sum(e["accepted"] for e in ev if e["step"] == "proposal"),
+            "lm_state_steps": [sum(e["lm_states"] for e in ev if e["step"] == "lm" and e["level"] == lv)
+                               for lv in (0, 1)],
+            "phases_s": {k: round(v, 4) for k, v in phase_split(log).items()}}
+
+
 # ---------------------------------------------------------------- ranks
 def replica_seed(seed, rank):
     """Each replica reconstructs its own scan: the synthetic seed moves with the rank."""
@@ -455,6 +486,7 @@ def main():
                     help="only time the sinc rigid transform of the scan size with STATES states")
     ap.add_argument("--operator-only", type=int, default=0, metavar="SHOTS",
                     help="only time encode / decode / encodedecode of the scan size with SHOTS shots")
+    ap.add_argument("--no-learned", action="store_true", help="skip the reconstruction with the learned proposal")
     args = ap.parse_args()
     cfg = SMALL if args.small else CFG
     if args.transform_only:
@@ -565,6 +597,10 @@ def main():
     e2e_clocks = eclk.stop()
     del Sd, yd, xh
 
+    # the same reconstruction with the learned motion proposal at the coarsest
+    # level (trained weights shipped with the package)
+    learned = learned_arm(ctx, sc, cfg, one_plain_s=ms * 1e-3, counts=None) if not args.no_learned else None
+
     # roofline of the dominant kernel family: the line passes of the sinc rigid
     # transform at full size (11 passes per forward transform, each reading
     # and writing the 64 state volumes)
@@ -614,6 +650,8 @@ def main():
                    "d2h_bytes_per_step": int(V * 8), "parts": {k: round(v, 4) for k, v in e2e_parts.items()},
                    "phases_s": {k: round(v, 4) for k, v in e2e_phases.items()}, "clocks": e2e_clocks},
            "roofline": roof}
+    if learned is not None:
+        out["learned"] = learned
     if rank == 0 and not args.no_cpu:
         est, thr, desc = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], counts)
         out["cpu_baseline"] = {"value": est, "unit": "s", "cores": thr, "kind": "port", "sample": desc}

@@ -73,6 +73,17 @@ SIGNATURES = [
     ("disorder_precondition_weights", C.c_int, [VP, VP, I32, C.c_int64, C.c_float, VP]),
     ("disorder_compress_coils", C.c_int, [VP, VP, I32, C.c_int64, VP, C.c_int64, C.c_double, I32, VP, VP,
                                           C.POINTER(I32), DP, DP]),
+    ("disorder_state_energies", C.c_int, [VP, VP, VP, VP, I32, VP, FP, I32, I32, DP]),
+    ("disorder_backproject_states", C.c_int, [VP, VP, VP, VP, I32, VP, FP, I32, I32, VP]),
+    ("disorder_net_param_count", C.c_int64, []),
+    ("disorder_net_create", C.c_int, [VP, C.POINTER(I32), I32, C.POINTER(VP)]),
+    ("disorder_net_destroy", C.c_int, [VP]),
+    ("disorder_net_set_params", C.c_int, [VP, VP, FP]),
+    ("disorder_net_get_params", C.c_int, [VP, VP, FP]),
+    ("disorder_net_forward", C.c_int, [VP, VP, VP, VP, I32, C.c_float, C.c_float, VP]),
+    ("disorder_net_backward", C.c_int, [VP, VP, VP, I32, VP, DP]),
+    ("disorder_net_adam", C.c_int, [VP, VP, VP, C.c_float, C.c_float, C.c_float, C.c_float, I32]),
+    ("disorder_propose_motion", C.c_int, [VP, VP, VP, VP, VP, I32, VP, FP, I32, I32, C.c_float, FP]),
 ]
 
 _lib = None

@@ -327,6 +327,73 @@ int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
   return DISORDER_OK;
 }
 
+// ---------------------------------------------------------------- per-state residuals
+int dis_state_residual(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* y, const float2* Sf, int C,
+                       const float2* x, const float* T, int n3_lo, int n3_hi, float2* r) {
+  const long long V = plan->V;
+  const int S = plan->n_mot;
+  const int N3 = plan->N[2];
+  const int N3c = n3_hi - n3_lo;
+  DIS_CUDA_TRY(cudaMemsetAsync(r, 0, sizeof(float2) * plan->n_samples * N3 * C, ctx->stream));
+  if (S == 0) return DISORDER_OK;
+  const size_t per = (size_t)V * sizeof(float2) + coil_slot_bytes(plan, C, N3c) + dis_table_bytes(plan, 1, false);
+  const int ch = (int)std::max<size_t>(1, std::min<size_t>(S, dis_budget_bytes() / per));
+  for (int c0 = 0; c0 < S; c0 += ch) {
+    const int n = std::min(ch, S - c0);
+    std::vector<int> st(n);
+    for (int j = 0; j < n; ++j) st[j] = c0 + j;
+    Workspace w;
+    DIS_TRY(dis_workspace(ctx, (size_t)n * per + (1 << 20), &w));
+    int* d_seg = nullptr;
+    DIS_TRY(dis_upload_ints(ctx, &w, st, &d_seg));
+    float2* z = w.take<float2>((size_t)n * V);
+    float2* A = w.take<float2>((size_t)n * C * plan->N[0] * plan->N[1] * N3c);
+    if (!z || !A) return dis_set_error(ctx, DISORDER_OOM, "state residual: workspace too small");
+    std::vector<SlotParams> prm;
+    dis_slot_params(T, S, st.data(), n, 1, &prm);
+    Tables tb;
+    DIS_TRY(dis_build_tables(ctx, plan, prm, false, &w, &tb));
+    DIS_TRY(dis_forward_transform(ctx, plan, x, 0, z, tb, 1, nullptr));
+    DIS_TRY(dis_encode_volumes(ctx, plan, z, d_seg, st, Sf, C, n3_lo, N3c, A, r, plan->n_samples, n3_lo, N3, y));
+  }
+  return DISORDER_OK;
+}
+
+int dis_backproject_states(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* r, const float2* Sf,
+                           int C, const float* T, float2* out) {
+  const long long V = plan->V;
+  const int S = plan->n_mot;
+  const int N3 = plan->N[2];
+  if (S == 0) return DISORDER_OK;
+  const int ch = dis_chunk_slots(plan, C, N3, 0, S);
+  Workspace ws;
+  DIS_TRY(dis_workspace(ctx, (size_t)ch * coil_slot_bytes(plan, C, N3) + dis_table_bytes(plan, ch, false) + 4096 * 4,
+                        &ws));
+  const float scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
+  for (int c0 = 0; c0 < S; c0 += ch) {
+    const int n = std::min(ch, S - c0);
+    Workspace w = ws;
+    std::vector<int> st(n);
+    for (int j = 0; j < n; ++j) st[j] = c0 + j;
+    int* d_seg = nullptr;
+    DIS_TRY(dis_upload_ints(ctx, &w, st, &d_seg));
+    float2* A = w.take<float2>((size_t)n * C * V);
+    if (!A) return dis_set_error(ctx, DISORDER_OOM, "back-projection: workspace too small");
+    float2* U = out + (long long)c0 * V;
+    CoilArgs ca = coil_args(plan, Sf, C, 0, N3, V, n, d_seg);
+    DIS_TRY(dis_coil_scatter_ifft2(ctx, plan, ca, r, plan->n_samples, 0, N3, nullptr, nullptr, A));
+    DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
+    if (dis_any_motion(T, S)) {
+      std::vector<SlotParams> prm;
+      dis_slot_params(T, S, st.data(), n, 0, &prm);
+      Tables tb;
+      DIS_TRY(dis_build_tables(ctx, plan, prm, false, &w, &tb));
+      DIS_TRY(dis_inverse_transform(ctx, plan, U, tb, 1, nullptr, 0.f));
+    }
+  }
+  return DISORDER_OK;
+}
+
 // ---------------------------------------------------------------- encodedecode
 int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const EncodeDecodeSpec& sp,
                               float2* out) {

@@ -52,6 +52,13 @@ int dis_encode_volumes(disorder_ctx_s* ctx, const disorder_plan_s* plan, const f
                        const std::vector<int>& segs, const float2* Sf, int C, int n3_lo, int N3c, float2* A, float2* y, long long y_ld,
                        int y_n3off, int y_N3, const float2* y_meas);
 int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const DecodeSpec& sp, float2* out);
+// r = encode(T_s x) - y for every motion state over readout rows [n3_lo, n3_hi),
+// the other rows zero (r: samples x N3 x C, encode's layout)
+int dis_state_residual(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* y, const float2* Sf, int C,
+                       const float2* x, const float* T, int n3_lo, int n3_hi, float2* r);
+// out[s] = T_s^H sum_c S_c^H F^H r_s for every motion state s (not summed)
+int dis_backproject_states(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* r, const float2* Sf,
+                           int C, const float* T, float2* out);
 int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const EncodeDecodeSpec& sp,
                               float2* out);
 int dis_gradient(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* x, long long x_s,

@@ -79,14 +79,19 @@ class ReconLog:
 
 def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), perc=16, resolMax=4.0,
                            nExtern=20, winit=1e-3, traLimXT=(0.05, 0.02), redFOV=1.0 / 3, echoesMin=4,
-                           tolerSolve=1e-3, log=None):
+                           tolerSolve=1e-3, log=None, proposal=None, levels=None):
     """Motion-corrected reconstruction of one scan on the GPU.
 
     S: coil maps (N1,N2,N3,C) device array; y: samples (Ns,N3,C) device array
     on the full k-space grid, ordered by shot as sample_lists(H) orders them
     (unitary DFT along the phase encodes, image space along the readout); H:
     (N1,N2) shot map, 1-based, DC first. perc: coil compression (count if >= 1,
-    energy share if < 1). Returns (x device volume, T (n_states, 6), log).
+    energy share if < 1). proposal: a proposal.MotionNet; at the motion levels
+    whose grid is its input size, each outer iteration first offers its
+    proposals and keeps those that lower a state's energy, then runs the LM
+    step from there (no counterpart in the reference). levels: run only
+    the first levels of the pyramid. Returns (x device volume, T (n_states, 6),
+    log).
     """
     log = log if log is not None else ReconLog()
     N = tuple(int(n) for n in N)
@@ -99,7 +104,7 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
     ctx.check(ctx.lib.disorder_memset(ctx.h, x.ptr, 0, x.nbytes))
     T = np.zeros((n_states, 6), np.float32)
     E = None
-    for l in range(L):
+    for l in range(L if levels is None else min(L, levels)):
         NXres = tuple(int(math.ceil(n * resPyr[l])) for n in N)
         # level operators (downsampleOperators, solveXT.m:333-342)
         xRes = api.resampling(x, NXres, ctx=ctx)
@@ -126,6 +131,7 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
         EH = api.Struct(Mbe=Mbe_d)
         A = api.Struct(Se=Se)
         est = bool(estT[l])
+        use_net = proposal is not None and est and tuple(NXres) == tuple(proposal.D)
         nReset, cont = 0, 0
         for n in range(nExtern):
             if nReset == 0 or cont % nReset == 0 or np.all(E.cT):  # solveXT.m:379-384
@@ -141,9 +147,16 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
             log.add(step="cg", level=l, it=n, iters=nn, tolType=tolType)
             if not est:
                 break
+            if use_net:
+                # a proposal that lowers a state's energy moves that state's
+                # motion; the LM step then runs from there for every state
+                from .proposal import propose_step
+                E, acc = propose_step(proposal, yRes, E, xRes, nF, ctx=ctx)
+                log.add(step="proposal", level=l, it=n, accepted=int(acc.sum()))
+            n_lm = int(np.sum(~np.asarray(E.cT, bool)))
             E = api.LMsolver(yRes, E, xRes, ctx=ctx)
             T = E.Tr
-            log.add(step="lm", level=l, it=n, unconverged=int(np.sum(~E.cT)),
+            log.add(step="lm", level=l, it=n, unconverged=int(np.sum(~E.cT)), lm_states=n_lm,
                     energy=float(np.sum(E.En)))
             if np.all(E.cT):  # weak convergence (solveXT.m:530-534)
                 est = False

@@ -207,6 +207,69 @@ int disorder_compress_coils(disorder_ctx ctx, const void* S, int32_t C_in, int64
                             int64_t n_y, double perc, int32_t C_max, void* S_out, void* y_out,
                             int32_t* C_out, double* D, double* U);
 
+/* ---- per-state residuals (the quantities LMsolver.m:72,82-93 forms per state) ----
+ * r = encode(T_s x) - y of every motion state s over the readout rows
+ * [n3_lo, n3_hi) (n3_hi <= 0: all rows).
+ * disorder_state_energies: En[s] = sum |r|^2 over state s's samples and
+ *   those rows / numel(y), the normalisation of LMsolver.m:82-83. En: host n_mot.
+ * disorder_backproject_states: out[s*V..] = T_s^H sum_c S_c^H F^H r_s, the
+ *   adjoint of state s alone (no sum over states). out: device n_mot volumes. */
+int disorder_state_energies(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
+                            int32_t n_coils, const void* x, const float* T, int32_t n3_lo,
+                            int32_t n3_hi, double* En);
+int disorder_backproject_states(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
+                                int32_t n_coils, const void* x, const float* T, int32_t n3_lo,
+                                int32_t n3_hi, void* out);
+
+/* ---- learned motion proposal (no counterpart in the reference) ----
+ * A 3-D convolutional network maps one state's back-projected residual and
+ * the current image (two complex volumes read as 4 channels: residual real
+ * and imaginary, image real and imaginary) to a 6-parameter motion update:
+ * 4 convolutions 3x3x3, stride 2, zero padding 1, with 16, 32,
+ * 64 and 64 output channels and GELU, a global average pool, and a
+ * 64 -> 128 (GELU) -> 6 perceptron. Weights are BF16 on the device (FP32
+ * master copy for training); activations and sums are FP32.
+ * Parameters, in this order (flat FP32): per convolution l the weights
+ * [tap = (kz*3 + ky)*3 + kx][c_in][c_out] and the bias [c_out]; then fc1
+ * [64][128] and its bias [128]; then fc2 [128][6] and its bias [6].
+ * Outputs 0-2 are translation updates / 2 in voxels of the input volume's
+ * grid and outputs 3-5 rotation updates / 8 degrees.
+ * D: input volume size (n1, n2, n3); max_batch: most volumes per call. */
+typedef struct disorder_net_s* disorder_net;
+int64_t disorder_net_param_count(void);
+int disorder_net_create(disorder_ctx ctx, const int32_t* D, int32_t max_batch, disorder_net* net);
+int disorder_net_destroy(disorder_net net);
+/* params: host FP32, disorder_net_param_count() values. */
+int disorder_net_set_params(disorder_ctx ctx, disorder_net net, const float* params);
+int disorder_net_get_params(disorder_ctx ctx, disorder_net net, float* params);
+/* in: device, batch complex volumes of size D (channels 0-1), multiplied by
+ * in_scale on read; ref: device, one complex volume shared by the batch
+ * (channels 2-3), multiplied by ref_scale, or NULL for zeros. Both must stay
+ * allocated until the backward of this forward. out: device batch x 6
+ * (row-major), or NULL to keep it internal. */
+int disorder_net_forward(disorder_ctx ctx, disorder_net net, const void* in, const void* ref,
+                         int32_t batch, float in_scale, float ref_scale, float* out);
+/* Gradient of loss = sum_b sum_k (out[b][k] - target[b][k])^2 / batch for the
+ * inputs of the last disorder_net_forward. target: device batch x 6.
+ * grad: device, param_count FP32 values (overwritten). loss: host. */
+int disorder_net_backward(disorder_ctx ctx, disorder_net net, const float* target, int32_t batch,
+                          float* grad, double* loss);
+/* One Adam step on the FP32 master parameters with grad (device), then the
+ * BF16 copies are refreshed. step: 1-based step count (bias correction). */
+int disorder_net_adam(disorder_ctx ctx, disorder_net net, const float* grad, float lr, float beta1,
+                      float beta2, float eps, int32_t step);
+/* Proposed motion update of every motion state: back-project the states'
+ * residuals at (x, T) over readout rows [n3_lo, n3_hi), run the network on
+ * them (scaled by gain / rms(x)) with x (scaled by 1 / rms(x)) and convert
+ * its outputs to T units
+ * (translations scaled by the plan's grid spacing rG[m][1] - rG[m][0], the
+ * full-grid voxels per volume voxel; rotations in radians).
+ * dT: host n_mot x 6, parameter-major like T (dT[p*n_mot + s]). The plan's
+ * volume size must equal the network's D. */
+int disorder_propose_motion(disorder_ctx ctx, disorder_plan plan, disorder_net net, const void* y,
+                            const void* Sf, int32_t n_coils, const void* x, const float* T,
+                            int32_t n3_lo, int32_t n3_hi, float gain, float* dT);
+
 #ifdef __cplusplus
 }
 #endif

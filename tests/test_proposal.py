@@ -1,0 +1,214 @@
+"""Learned motion proposal: the oracle network (CPU) and the library's
+network kernels, per-state back-projections and energies (GPU) against it.
+
+Tolerances: the device computes in FP32 with the BF16 weights the oracle
+also uses, so the forward outputs match the FP64 oracle to 1e-5 relative;
+gradients, summed with FP32 atomics in arbitrary order, to 1e-4. Per-state
+back-projections and energies are FP32 encoding-path results (1e-5)."""
+
+import numpy as np
+import pytest
+
+from conftest import make_problem
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-30))
+
+
+# ---------------------------------------------------------------- CPU
+def test_oracle_gradient_matches_finite_differences():
+    from oracle import proposal as op
+    rng = np.random.default_rng(0)
+    p = op.init_params(rng).astype(np.float64)
+    x = rng.standard_normal((2, 12, 16, 16, 4))
+    t = rng.standard_normal((2, 6)) * 0.3
+    G, _ = op.grad(p, x, t, rnd=False)
+    conv, (f1w, f1b, f2w, f2b), P = op.layout()
+    picks = [0, 5, conv[0][1] + 3, conv[1][0] + 77, conv[2][0] + 4000, conv[3][0] + 9000, conv[3][1] + 1,
+             f1w + 3, f1b + 7, f2w + 11, f2b + 2]
+    for i in picks:
+        e = 1e-6 * max(1.0, abs(p[i]))
+        pp, pm = p.copy(), p.copy()
+        pp[i] += e
+        pm[i] -= e
+        fd = (op.loss(pp, x, t, rnd=False) - op.loss(pm, x, t, rnd=False)) / (2 * e)
+        assert abs(G[i] - fd) <= 1e-6 * max(abs(fd), 1e-3), (i, G[i], fd)
+
+
+def test_oracle_bf16_rounding_is_nearest_even():
+    from oracle.proposal import bf16_round
+    v = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -9, -2.5, 1e-30], np.float32)
+    r = bf16_round(v)
+    assert r[0] == 1.0 and r[1] == 1.0  # tie to even
+    assert r[2] == np.float32(1.0 + 2 ** -7)
+    assert r[3] == -2.5
+    assert (r.view(np.uint32) & 0xFFFF == 0).all()
+
+
+def test_parameter_layout_matches_the_library():
+    import os
+    from disorder_b200 import _lib
+    from oracle import proposal as op
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libdisorder.so not built")
+    assert int(_lib.load().disorder_net_param_count()) == op.param_count() == 190710
+
+
+def test_host_init_matches_the_layout():
+    from disorder_b200 import proposal as pr
+    from oracle import proposal as op
+    import os
+    from disorder_b200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libdisorder.so not built")
+    p = pr.init_params(np.random.default_rng(3))
+    assert p.dtype == np.float32 and p.size == op.param_count()
+    conv, (f1w, f1b, f2w, f2b), _ = op.layout()
+    for l, (w, b) in enumerate(conv):
+        assert p[w:b].std() > 0 and not p[b:b + op.CH[l + 1]].any()
+    assert not p[f1b:f2w].any() and not p[f2b:].any()
+
+
+# ---------------------------------------------------------------- GPU
+@pytest.fixture(scope="module")
+def ctx():
+    import disorder_b200 as db
+    return db.Context(0)
+
+
+def _net_case(seed, D=(24, 20, 16), B=3):
+    from oracle import proposal as op
+    rng = np.random.default_rng(seed)
+    vols = (rng.standard_normal((B,) + D) + 1j * rng.standard_normal((B,) + D)).astype(np.complex64)
+    ref = (rng.standard_normal(D) + 1j * rng.standard_normal(D)).astype(np.complex64)
+    p = op.init_params(rng)
+    t = (0.5 * rng.standard_normal((B, 6))).astype(np.float32)
+    return vols, ref, p, t
+
+
+def _dev_vols(ctx, vols):
+    return ctx.upload(np.moveaxis(vols, 0, -1))
+
+
+@pytest.mark.gpu
+def test_net_forward_matches_oracle(ctx):
+    from disorder_b200 import proposal as pr
+    from oracle import proposal as op
+    D = (24, 20, 16)
+    vols, ref, p, _ = _net_case(1, D)
+    net = pr.MotionNet(ctx, D, 4, params=p)
+    out = net.forward(_dev_vols(ctx, vols), ctx.upload(ref), 3, 0.8, 1.3)
+    want, _ = op.forward(p, op.features(vols, ref, 0.8, 1.3))
+    assert rel(out, want) < 1e-5
+    # no reference volume: channels 2-3 read zeros
+    out0 = net.forward(_dev_vols(ctx, vols), None, 3, 0.8, 1.3)
+    want0, _ = op.forward(p, op.features(vols, None, 0.8))
+    assert rel(out0, want0) < 1e-5
+
+
+@pytest.mark.gpu
+def test_net_gradient_matches_oracle(ctx):
+    from disorder_b200 import proposal as pr
+    from oracle import proposal as op
+    D = (24, 20, 16)
+    vols, ref, p, t = _net_case(2, D)
+    net = pr.MotionNet(ctx, D, 4, params=p)
+    net.forward(_dev_vols(ctx, vols), ctx.upload(ref), 3, 0.8, 1.3)
+    grad = ctx.empty((net.P,), np.float32)
+    loss = net.backward(ctx.upload(t.T.copy(order="F")), 3, grad)
+    f = op.features(vols, ref, 0.8, 1.3)
+    G, _ = op.grad(p, f, t)
+    g = grad.numpy()
+    assert abs(loss - op.loss(p, f, t)) < 1e-5 * max(1.0, loss)
+    conv, (f1w, f1b, f2w, f2b), P = op.layout()
+    blocks = [(w, b) for w, b in conv] + [(b, b + op.CH[l + 1]) for l, (w, b) in enumerate(conv)]
+    blocks += [(f1w, f1b), (f1b, f2w), (f2w, f2b), (f2b, P)]
+    errs = {(a, b): rel(g[a:b], G[a:b]) for a, b in blocks}
+    assert max(errs.values()) < 1e-4, errs
+
+
+@pytest.mark.gpu
+def test_adam_lowers_the_loss_and_keeps_master_weights(ctx):
+    from disorder_b200 import proposal as pr
+    D = (24, 20, 16)
+    vols, ref, p, t = _net_case(3, D)
+    net = pr.MotionNet(ctx, D, 4, params=p)
+    v = _dev_vols(ctx, vols)
+    r = ctx.upload(ref)
+    tg = ctx.upload(t.T.copy(order="F"))
+    grad = ctx.empty((net.P,), np.float32)
+    losses = []
+    for _ in range(40):
+        net.forward(v, r, 3, 0.8, 1.3)
+        losses.append(net.backward(tg, 3, grad))
+        net.adam(grad, 3e-3)
+    assert losses[-1] < 0.2 * losses[0], losses[::8]
+    assert not np.array_equal(net.get_params(), p)
+
+
+def _device_problem(ctx, N=(24, 20, 16), C=3, S=4, seed=11):
+    import disorder_b200 as db
+    from oracle import encoding as oe
+    sc, Eo = make_problem(N, C, S, seed=seed, rot_deg=4.0, trans=2.0)
+    sc.y = oe.encode(sc.x_gt.astype(np.complex128), Eo).astype(np.complex64)  # samples at the true motion
+    cent = [np.ceil((n + 1) / 2.0) for n in N]
+    E = db.Struct(Tr=sc.T_gt * 0.5, NMs=S, NSe=S + 1, Sf=ctx.upload(sc.S.astype(np.complex64)),
+                  grids=db.generateTransformGrids(N, N, cent, sh=1), ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt)
+    Eo.Tr = (sc.T_gt * 0.5).astype(np.float32)
+    rng = np.random.default_rng(seed + 1)
+    x = (sc.x_gt + 0.05 * (rng.standard_normal(N) + 1j * rng.standard_normal(N))).astype(np.complex64)
+    return sc, E, Eo, x
+
+
+def _oracle_residual(sc, Eo, x, lo, hi):
+    from oracle import encoding as oe
+    r = oe.encode(x.astype(np.complex128), Eo) - sc.y.astype(np.complex128)
+    r[:, :lo] = 0
+    r[:, hi:] = 0
+    return r
+
+
+@pytest.mark.gpu
+def test_backproject_states_matches_oracle(ctx):
+    from disorder_b200 import proposal as pr
+    from oracle import encoding as oe
+    from oracle.transform import precomputeFactorsSincRigidTransform, sincRigidTransform
+    sc, E, Eo, x = _device_problem(ctx)
+    lo, hi = 0, 11
+    S = E.NMs
+    out = pr.backproject_states(ctx.upload(sc.y.astype(np.complex64)), E, x, np.arange(lo, hi), ctx=ctx).numpy()
+    r = _oracle_residual(sc, Eo, x, lo, hi)
+    xo = oe._decode_states(r, Eo, None, list(range(S)), "fft")
+    et, _ = precomputeFactorsSincRigidTransform(Eo.grids, np.asarray(Eo.Tr), 0, 0)
+    ref = sincRigidTransform(xo, et, 0, sumR=0)[:, :, :, 0, :]
+    for s in range(S):
+        assert rel(out[..., s], ref[..., s]) < 1e-5, s
+
+
+@pytest.mark.gpu
+def test_state_energies_match_oracle(ctx):
+    from disorder_b200 import proposal as pr
+    sc, E, Eo, x = _device_problem(ctx, seed=12)
+    lo, hi = 2, 13
+    En = pr.state_energies(ctx.upload(sc.y.astype(np.complex64)), E, x, np.arange(lo, hi), ctx=ctx)
+    r = _oracle_residual(sc, Eo, x, lo, hi)
+    n = r.size
+    ref = [np.sum(np.abs(r[int(sc.nEc[s]):int(sc.nEc[s + 1])]) ** 2) / n for s in range(E.NMs)]
+    assert rel(En, ref) < 1e-5
+
+
+@pytest.mark.gpu
+def test_propose_step_never_raises_a_state_energy(ctx):
+    from disorder_b200 import proposal as pr
+    sc, E, Eo, x = _device_problem(ctx, N=(32, 32, 24), seed=13)
+    E = E.copy(cT=np.zeros(E.NMs, bool))
+    y = ctx.upload(sc.y.astype(np.complex64))
+    net = pr.MotionNet(ctx, (32, 32, 24), 8, params=pr.init_params(np.random.default_rng(4)))
+    nF = np.arange(0, 16)
+    En0 = pr.state_energies(y, E, x, nF, ctx=ctx)
+    E1, acc = pr.propose_step(net, y, E, x, nF, ctx=ctx)
+    En1 = pr.state_energies(y, E1, x, nF, ctx=ctx)
+    assert np.all(En1[acc] < En0[acc])
+    assert np.array_equal(np.asarray(E1.Tr)[~acc], np.asarray(E.Tr)[~acc])
