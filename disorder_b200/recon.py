@@ -6,9 +6,10 @@ Fourier-cropped image, coils and samples (downsampleOperators, :333-342),
 then outer iterations of CGsolver (:431) and LMsolver (:507) with the
 reference's motion-convergence resets (:379-388) and, once the motion has
 converged or at the last level, a final CGsolver to the energy tolerance
-(:414-425, nIt=300, 'Energy', tolerSolve). Outlier weighting, Haar binning of
-motion states (compressMotion), NIfTI output and the Gibbs/B-spline filters
-of the reference driver are not part of this path.
+(:414-425, nIt=300, 'Energy', tolerSolve). Before every image update the
+motion states are binned by compressMotion (:392). Outlier weighting, NIfTI
+output and the Gibbs/B-spline filters of the reference driver are not part
+of this path.
 """
 
 import math
@@ -67,6 +68,81 @@ def level_sampling(H, n_states, NYres):
     return ky.astype(np.int32), kz.astype(np.int32), nEc, np.concatenate(seg), row_of[Lf[lin]]
 
 
+def _haar_dec(x, levels):
+    """Multi-level orthonormal Haar decomposition with half-point symmetric
+    extension at odd lengths (the pair (x[n-1], x[n-1])): returns the
+    coefficient list [a_L, d_L, ..., d_1] and the length of each level."""
+    a = np.asarray(x, np.float64)
+    details, lengths = [], [a.size]
+    s = math.sqrt(0.5)
+    for _ in range(levels):
+        if a.size % 2:
+            a = np.append(a, a[-1])
+        details.append((a[0::2] - a[1::2]) * s)
+        a = (a[0::2] + a[1::2]) * s
+        lengths.append(a.size)
+    return [a] + details[::-1], lengths
+
+
+def _haar_rec(coefs, lengths):
+    s = math.sqrt(0.5)
+    a = coefs[0]
+    for j, d in enumerate(coefs[1:]):
+        x = np.empty(2 * a.size)
+        x[0::2] = (a + d) * s
+        x[1::2] = (a - d) * s
+        a = x[:lengths[-2 - j]]
+    return a
+
+
+def compressMotion(T, nEc, res, traLimX=(0.05, 0.02)):
+    """Methods/compressMotion.m:19-80: bin the motion states for the image
+    update. Each parameter's trajectory over the states is Haar-decomposed
+    (floor(log2(n)) levels, :30-33), coefficients below the binning limit
+    (traLimX(1)*res voxels, traLimX(2)*res degrees, :32) are zeroed, and the
+    trajectory is rebuilt (:34-35). Runs of consecutive states whose rebuilt
+    transforms agree to 1e-6 form one bin (:40-53) with the mean transform
+    (:56-65); their samples, consecutive already, form one segment. The outer
+    segments follow unchanged (:66-72).
+    T: (n, 6); nEc: offsets of the n motion segments then the outer ones.
+    Returns (T_bins (nb, 6) float32, nEc of the bins then the outer
+    segments, bin of each state)."""
+    T = np.asarray(T, np.float64)
+    n = T.shape[0]
+    nEc = np.asarray(nEc, np.int64)
+    if n <= 1:
+        return T.astype(np.float32), nEc.copy(), np.zeros(n, np.int64)
+    levels = int(math.floor(math.log2(n)))
+    Test = np.empty_like(T)
+    for m in range(6):
+        th = traLimX[0] * res if m < 3 else math.radians(traLimX[1] * res)
+        C, L = _haar_dec(T[:, m], levels)
+        C = [np.where(np.abs(c) < th, 0.0, c) for c in C]
+        Test[:, m] = _haar_rec(C, L)
+    bins = np.zeros(n, np.int64)
+    starts = [0]
+    for s in range(1, n):
+        if np.any(np.abs(Test[s] - Test[starts[-1]]) > 1e-6):
+            starts.append(s)
+        bins[s] = len(starts) - 1
+    starts.append(n)
+    Tb = np.stack([Test[a:b].mean(axis=0) for a, b in zip(starts[:-1], starts[1:])])
+    off = np.concatenate([nEc[starts], nEc[n + 1:]])
+    return Tb.astype(np.float32), off, bins
+
+
+def binned(E, res, traLimX=(0.05, 0.02)):
+    """E with its motion states binned by compressMotion (solveXT.m:392): the
+    structure for the image update; the motion update keeps E itself
+    (solveXT.m:495)."""
+    Tb, off, _ = compressMotion(E.Tr, E.nEc, res, traLimX)
+    nb = Tb.shape[0]
+    if nb == E.NMs:
+        return E.copy(Tr=Tb)
+    mSt = np.repeat(np.arange(len(off) - 1, dtype=np.int32), np.diff(off))
+    return E.copy(Tr=Tb, NMs=nb, NSe=len(off) - 1, nEc=off, mSt=mSt, plan_cache=None)
+
+
 class ReconLog:
     def __init__(self):
         self.events = []
@@ -79,7 +155,7 @@ class ReconLog:
 
 def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), perc=16, resolMax=4.0,
                            nExtern=20, winit=1e-3, traLimXT=(0.05, 0.02), redFOV=1.0 / 3, echoesMin=4,
-                           tolerSolve=1e-3, log=None, proposal=None, levels=None):
+                           tolerSolve=1e-3, log=None, proposal=None, levels=None, traLimX=(0.05, 0.02)):
     """Motion-corrected reconstruction of one scan on the GPU.
 
     S: coil maps (N1,N2,N3,C) device array; y: samples (Ns,N3,C) device array
@@ -90,7 +166,8 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
     whose grid is its input size, each outer iteration first offers its
     proposals and keeps those that lower a state's energy, then runs the LM
     step from there (no counterpart in the reference). levels: run only
-    the first levels of the pyramid. Returns (x device volume, T (n_states, 6),
+    the first levels of the pyramid. traLimX: motion binning limits of the
+    image update (compressMotion; None: no binning). Returns (x device volume, T (n_states, 6),
     log).
     """
     log = log if log is not None else ReconLog()
@@ -143,8 +220,9 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
                 nX, tolType, tol = 1, "RelativeResidual2Error", 0.0  # nIt(2)=1 at motion levels
             else:
                 nX, tolType, tol = 300, "Energy", tolerSolve
-            xRes, EnX, nn = api.CGsolver(yRes, E, EH, A, None, None, xRes, nX, tolType, tol, ctx=ctx)
-            log.add(step="cg", level=l, it=n, iters=nn, tolType=tolType)
+            Ex = binned(E, resIso[-1], traLimX) if traLimX is not None else E  # solveXT.m:392
+            xRes, EnX, nn = api.CGsolver(yRes, Ex, EH, A, None, None, xRes, nX, tolType, tol, ctx=ctx)
+            log.add(step="cg", level=l, it=n, iters=nn, tolType=tolType, states=int(Ex.NMs))
             if not est:
                 break
             if use_net:
