@@ -74,6 +74,7 @@ SIGNATURES = [
     ("disorder_compress_coils", C.c_int, [VP, VP, I32, C.c_int64, VP, C.c_int64, C.c_double, I32, VP, VP,
                                           C.POINTER(I32), DP, DP]),
     ("disorder_state_energies", C.c_int, [VP, VP, VP, VP, I32, VP, FP, I32, I32, DP]),
+    ("disorder_sample_energies", C.c_int, [VP, VP, VP, VP, I32, VP, FP, VP, DP]),
     ("disorder_backproject_states", C.c_int, [VP, VP, VP, VP, I32, VP, FP, I32, I32, VP]),
     ("disorder_net_param_count", C.c_int64, []),
     ("disorder_net_create", C.c_int, [VP, C.POINTER(I32), I32, C.POINTER(VP)]),

@@ -361,6 +361,27 @@ def computeEnergy(y, x, E, R=None, EH=None, ctx=None):
     return np.array([En[0], En[1]])
 
 
+def sampleEnergies(y, x, E, EH=None, ctx=None):
+    """Reconstruction/computeEnergy.m:34-80 with avdi=1 (solveXT.m:443): per
+    sample, the sum over readout rows (weighted by EH.Mb and EH.Mbe) and
+    coils of |encode(x) - y|^2. Returns (n_samples,) float64."""
+    ctx = ctx or default_context()
+    p = _plan(E, ctx)
+    yd, _ = _dev(ctx, y, np.complex64)
+    xd, _ = _dev(ctx, x, np.complex64)
+    Sd, _ = _dev(ctx, E.Sf, np.complex64)
+    Cn = Sd.shape[3] if len(Sd.shape) > 3 else 1
+    ws = [getattr(EH, f) for f in ("Mb", "Mbe") if EH is not None and EH.has(f)]
+    if len(ws) == 2:  # sqrt(Mb) and sqrt(Mbe) both weight the residual (computeEnergy.m:36-37)
+        ws = [np.prod([w.numpy() if isinstance(w, DeviceArray) else np.asarray(w) for w in ws], axis=0)]
+    Mbe, _ = _dev(ctx, ws[0] if ws else None, np.float32)
+    En = np.zeros(max(p.n_samples, 1))
+    T = _T(E)
+    ctx.check(ctx.lib.disorder_sample_energies(ctx.h, p.h, yd.ptr, Sd.ptr, Cn, xd.ptr, T[1] if T else None,
+                                               Mbe.ptr if Mbe else None, En.ctypes.data_as(_lib.DP)))
+    return En[:p.n_samples]
+
+
 TOLTYPES = {"RelativeResidual2Error": 1, "Energy": 6, "None": 7}
 
 

@@ -1,7 +1,8 @@
 // Learned motion proposal: a small 3-D convolutional network that maps one
 // motion state's back-projected k-space residual to a 6-parameter motion
 // update, with its forward, backward and Adam kernels, plus the per-state
-// residual entry points it is fed by. There is no counterpart in the
+// residual entry points it is fed by and the per-sample residual energies of
+// the driver's outlier weighting. There is no counterpart in the
 // reference; the plain Levenberg-Marquardt step (LMsolver.m) stays the judge
 // of every proposal (the caller accepts a proposal only where the state's
 // energy drops).
@@ -414,6 +415,22 @@ __global__ void transpose_kernel(const bf16* __restrict__ w, bf16* __restrict__ 
 
 // network outputs -> T units: translations times the grid spacing of each
 // axis (full-grid voxels per volume voxel), rotations to radians
+// out[i] = sum over readout rows and coils of wrow[n3] |r[i, n3, c]|^2
+__global__ void sample_energy_kernel(const float2* __restrict__ r, long long ns, int N3, int C,
+                                     const float* __restrict__ wrow, double* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ns) return;
+  double s = 0.0;
+  for (int c = 0; c < C; ++c)
+    for (int n3 = 0; n3 < N3; ++n3) {
+      const float w = wrow ? wrow[n3] : 1.f;
+      if (w == 0.f) continue;
+      const float2 v = r[i + ns * (n3 + (long long)N3 * c)];
+      s += (double)w * ((double)v.x * v.x + (double)v.y * v.y);
+    }
+  out[i] = s;
+}
+
 __global__ void convert_out_kernel(const float* __restrict__ out, int n, float sp0, float sp1, float sp2,
                                    float* __restrict__ dT) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -773,6 +790,39 @@ int disorder_state_energies(disorder_ctx ctx, disorder_plan plan, const void* y,
   DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   const double NElY = (double)plan->n_samples * plan->N[2] * n_coils;
   for (int s = 0; s < S; ++s) En[s] = sums[(size_t)s * 28] / NElY;
+  return DISORDER_OK;
+}
+
+int disorder_sample_energies(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf, int32_t n_coils,
+                             const void* x, const float* T, const float* Mbe, double* En) {
+  if (!ctx) return DISORDER_BAD_ARG;
+  if (!plan || plan->ctx != ctx) return dis_set_error(ctx, DISORDER_BAD_ARG, "bad plan");
+  if (!y || !Sf || !x || !En || n_coils < 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "sample energies: bad arguments");
+  DIS_CUDA_TRY(cudaSetDevice(ctx->device));
+  const long long ns = plan->n_samples;
+  Workspace sw;
+  float2* r = residual_buffer(ctx, plan, n_coils, ns * sizeof(double) + 256, &sw);
+  double* d_en = sw.take<double>(std::max<long long>(ns, 1));
+  if (!r || !d_en) return dis_set_error(ctx, DISORDER_OOM, "sample energies: no residual buffer");
+  EncodeSpec sp;
+  sp.x = (const float2*)x;
+  sp.Sf = (const float2*)Sf;
+  sp.C = n_coils;
+  sp.T = T;
+  sp.T_n = plan->n_mot;
+  for (int s = 0; s < plan->n_seg; ++s) sp.segs.push_back(s);
+  sp.n3_lo = 0;
+  sp.N3c = plan->N[2];
+  sp.y_ld = ns;
+  sp.y_n3off = 0;
+  sp.y_N3 = plan->N[2];
+  DIS_TRY(dis_encode_segments(ctx, plan, sp, r, (const float2*)y));
+  if (ns == 0) return DISORDER_OK;
+  sample_energy_kernel<<<blocks(ns), 256, 0, ctx->stream>>>(r, ns, plan->N[2], n_coils, Mbe, d_en);
+  dis_count(ctx);
+  DIS_CUDA_TRY(cudaGetLastError());
+  DIS_CUDA_TRY(cudaMemcpyAsync(En, d_en, sizeof(double) * ns, cudaMemcpyDeviceToHost, ctx->stream));
+  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return DISORDER_OK;
 }
 

@@ -7,9 +7,10 @@ then outer iterations of CGsolver (:431) and LMsolver (:507) with the
 reference's motion-convergence resets (:379-388) and, once the motion has
 converged or at the last level, a final CGsolver to the energy tolerance
 (:414-425, nIt=300, 'Energy', tolerSolve). Before every image update the
-motion states are binned by compressMotion (:392). Outlier weighting, NIfTI
-output and the Gibbs/B-spline filters of the reference driver are not part
-of this path.
+motion states are binned by compressMotion (:392); the final image update
+weights the shots by the outlier rejection of the last motion level
+(:440-482). NIfTI output, the CS/shearlet reconstruction and the
+Gibbs/B-spline filters of the reference driver are not part of this path.
 """
 
 import math
@@ -143,6 +144,38 @@ def binned(E, res, traLimX=(0.05, 0.02)):
     return E.copy(Tr=Tb, NMs=nb, NSe=len(off) - 1, nEc=off, mSt=mSt, plan_cache=None)
 
 
+def outlier_weights(Re, sweeps, n_sweeps, leff, percRobustShot=(0.125, 0.25), enerRobustShot=0.95):
+    """Shot weights of the outlier rejection (Reconstruction/solveXT.m:447-466).
+    Re: per-sample residual energies (computeEnergy with avdi=1); sweeps: the
+    shot of every sample (n_sweeps and above: outer samples, ignored).
+    Percentiles of each shot's log residuals (MATLAB prctile, the midpoint
+    rule) are standardised by a robust spread taken from the lower
+    percentiles across shots; a shot's weight is the tail probability of its
+    mean score over (1 - enerRobustShot) / n_sweeps, capped at 1."""
+    from statistics import NormalDist
+    nd = NormalDist()
+    Re = np.maximum(np.asarray(Re, np.float64), np.finfo(np.float64).tiny)
+    sweeps = np.asarray(sweeps)
+    lo, hi = (0.15, 0.85) if leff > 0 else (0.3, 0.7)
+    percUse = 100 * np.round(np.arange(lo, hi + 1e-9, 0.05), 10)
+    WeO = np.zeros((n_sweeps, percUse.size))
+    for s in range(n_sweeps):
+        v = np.log(Re[sweeps == s])
+        WeO[s] = np.percentile(v, percUse, method="hazen") if v.size else 0.0
+    pr = np.asarray(percRobustShot, np.float64)
+    q = np.percentile(WeO, 100 * pr, axis=0, method="hazen")
+    Westd = (q[1] - q[0]) / (nd.inv_cdf(pr[1]) - nd.inv_cdf(pr[0]))
+    pm = float(pr.mean())
+    # the centre sits -norminv(pm) spreads above the pm-th percentile; the
+    # reference adds sqrt(2)*erfcinv(2*pm)*Westd, the same quantity (:462)
+    Wmea = np.percentile(WeO, 100 * pm, axis=0, method="hazen") - Westd * nd.inv_cdf(pm)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        z = np.mean((WeO - Wmea) / Westd, axis=1)
+    z = np.where(np.isfinite(z), z, -np.inf)
+    tail = np.array([1.0 - nd.cdf(v) if np.isfinite(v) else 1.0 for v in z])
+    return np.minimum(tail / ((1.0 - enerRobustShot) / n_sweeps), 1.0)
+
+
 class ReconLog:
     def __init__(self):
         self.events = []
@@ -155,7 +188,7 @@ class ReconLog:
 
 def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), perc=16, resolMax=4.0,
                            nExtern=20, winit=1e-3, traLimXT=(0.05, 0.02), redFOV=1.0 / 3, echoesMin=4,
-                           tolerSolve=1e-3, log=None, proposal=None, levels=None, traLimX=(0.05, 0.02)):
+                           tolerSolve=1e-3, log=None, proposal=None, levels=None, traLimX=(0.05, 0.02), outliers=True):
     """Motion-corrected reconstruction of one scan on the GPU.
 
     S: coil maps (N1,N2,N3,C) device array; y: samples (Ns,N3,C) device array
@@ -167,8 +200,10 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
     proposals and keeps those that lower a state's energy, then runs the LM
     step from there (no counterpart in the reference). levels: run only
     the first levels of the pyramid. traLimX: motion binning limits of the
-    image update (compressMotion; None: no binning). Returns (x device volume, T (n_states, 6),
-    log).
+    image update (compressMotion; None: no binning). outliers: the shot
+    weights of the outlier rejection (rec.Alg.AlignedRec=2, solveXT.m:440-482)
+    from the last motion level at full in-plane sampling, applied in the final
+    image update. Returns (x device volume, T (n_states, 6), log).
     """
     log = log if log is not None else ReconLog()
     N = tuple(int(n) for n in N)
@@ -181,7 +216,10 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
     ctx.check(ctx.lib.disorder_memset(ctx.h, x.ptr, 0, x.nbytes))
     T = np.zeros((n_states, 6), np.float32)
     E = None
+    n_coarse = int(np.sum(resPyr != 1))
+    We_shot = None
     for l in range(L if levels is None else min(L, levels)):
+        leff = l + 1 - n_coarse  # solveXT.m:269
         NXres = tuple(int(math.ceil(n * resPyr[l])) for n in N)
         # level operators (downsampleOperators, solveXT.m:333-342)
         xRes = api.resampling(x, NXres, ctx=ctx)
@@ -206,6 +244,12 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
                        mSt=mSt, w=np.full(n_states, winit, np.float32), cT=cT0.copy(), winit=winit,
                        tL=list(np.asarray(traLimXT) * resIso[l]), nF=nF)
         EH = api.Struct(Mbe=Mbe_d)
+        if not estT[l] and leff > 0 and We_shot is not None and np.any(We_shot < 1):
+            # soft shot weights in the final image update (solveXT.m:411-415)
+            wsmp = np.ones(len(mSt), np.float32)
+            inner = mSt < n_states
+            wsmp[inner] = We_shot[mSt[inner]]
+            EH = api.Struct(Mbe=Mbe_d, We=wsmp)
         A = api.Struct(Se=Se)
         est = bool(estT[l])
         use_net = proposal is not None and est and tuple(NXres) == tuple(proposal.D)
@@ -225,6 +269,11 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
             log.add(step="cg", level=l, it=n, iters=nn, tolType=tolType, states=int(Ex.NMs))
             if not est:
                 break
+            if outliers and leff >= 0:
+                # residual energy per sample and outlier detection (solveXT.m:440-466)
+                Re = api.sampleEnergies(yRes, xRes, Ex, EH, ctx=ctx)
+                We_shot = outlier_weights(Re, mSt, n_states, leff)
+                log.add(step="outliers", level=l, it=n, rejected=int(np.sum(We_shot < 1)))
             if use_net:
                 # a proposal that lowers a state's energy moves that state's
                 # motion; the LM step then runs from there for every state

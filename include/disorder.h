@@ -217,6 +217,15 @@ int disorder_compress_coils(disorder_ctx ctx, const void* S, int32_t C_in, int64
 int disorder_state_energies(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
                             int32_t n_coils, const void* x, const float* T, int32_t n3_lo,
                             int32_t n3_hi, double* En);
+/* [Re]=computeEnergy(y,x,E,[],EH,[],[],[],[],1) (Reconstruction/computeEnergy.m:34-80,
+ * no=2, avdi=1), the per-sample residual energies of the outlier weighting
+ * (Reconstruction/solveXT.m:443): En[i] = sum over readout rows and coils of
+ * Mbe[n3] |encode(x) - y|^2 for every sample i (all segments). Mbe: device
+ * length N3 readout weights (EH.Mbe, or EH.Mb.*EH.Mbe when both are set) or
+ * NULL (all ones). En: host n_samples doubles. */
+int disorder_sample_energies(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
+                             int32_t n_coils, const void* x, const float* T, const float* Mbe,
+                             double* En);
 int disorder_backproject_states(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
                                 int32_t n_coils, const void* x, const float* T, int32_t n3_lo,
                                 int32_t n3_hi, void* out);

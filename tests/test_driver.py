@@ -76,3 +76,59 @@ def test_pyramid_plan_of_the_benchmark_scan():
     resPyr, L, estT, resIso = recon.pyramidPlan((1.0, 1.0, 1.0), 4.0, 1, (1, 0))
     assert L == 3 and list(resPyr) == [0.25, 0.5, 1.0] and list(estT) == [1, 1, 0]
     assert np.allclose(resIso, math.sqrt(2) * np.array([4, 2, 1]))
+
+
+# ---------------------------------------------------------------- outlier rejection
+def test_prctile_is_the_midpoint_rule():
+    x = np.array([4.0, 1.0, 3.0, 2.0])
+    # MATLAB prctile: sorted values sit at 100*(i-0.5)/n, linear in between, clamped
+    assert np.percentile(x, 50, method="hazen") == 2.5
+    assert np.percentile(x, 10, method="hazen") == 1.0
+    assert np.percentile(x, 25, method="hazen") == 1.5
+
+
+def _shot_residuals(rng, n_shots=64, per=64, bad=()):
+    Re = np.exp(rng.normal(0.0, 0.3, n_shots * per))
+    sweeps = np.repeat(np.arange(n_shots), per)
+    for b in bad:
+        Re[sweeps == b] *= 50.0
+    return Re, sweeps
+
+
+def test_no_outliers_keep_unit_weights():
+    Re, sw = _shot_residuals(np.random.default_rng(3))
+    We = recon.outlier_weights(Re, sw, 64, leff=1)
+    assert We.shape == (64,) and np.all(We == 1.0)
+
+
+def test_corrupted_shots_are_down_weighted():
+    Re, sw = _shot_residuals(np.random.default_rng(4), bad=(5, 40))
+    sw = np.concatenate([sw, np.full(30, 64)])  # outer samples are ignored
+    Re = np.concatenate([Re, np.full(30, 1e6)])
+    We = recon.outlier_weights(Re, sw, 64, leff=1)
+    assert We[5] < 1e-3 and We[40] < 1e-3
+    assert np.all(np.delete(We, [5, 40]) == 1.0)
+
+
+@pytest.mark.gpu
+def test_sample_energies_match_oracle():
+    import disorder_b200 as db
+    from conftest import make_problem
+    from oracle import encoding as oe
+    from oracle.encoding import Struct as OStruct
+    N, C, S = (24, 20, 16), 3, 4
+    sc, Eo = make_problem(N, C, S, seed=21, rot_deg=4.0, trans=2.0)
+    rng = np.random.default_rng(22)
+    y = (oe.encode(sc.x_gt.astype(np.complex128), Eo)
+         + 0.01 * (rng.standard_normal((int(sc.nEc[-1]), N[2], C)) + 0j)).astype(np.complex64)
+    x = (sc.x_gt * 0.9).astype(np.complex64)
+    Mb = rng.uniform(0.5, 1.0, N[2]).astype(np.float32)
+    Mbe = (np.arange(N[2]) < 11).astype(np.float32)
+    ctx = db.Context(0)
+    cent = [np.ceil((n + 1) / 2.0) for n in N]
+    E = db.Struct(Tr=sc.T_gt, NMs=S, NSe=S + 1, Sf=ctx.upload(sc.S.astype(np.complex64)),
+                  grids=db.generateTransformGrids(N, N, cent, sh=1), ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt)
+    got = db.api.sampleEnergies(y, x, E, db.Struct(Mb=Mb, Mbe=ctx.upload(Mbe)), ctx=ctx)
+    ref = oe.computeEnergy(y.astype(np.complex128), x.astype(np.complex128), Eo, EH=OStruct(Mb=Mb, Mbe=Mbe),
+                           per_sample=True)
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
