@@ -212,3 +212,26 @@ def test_propose_step_never_raises_a_state_energy(ctx):
     En1 = pr.state_energies(y, E1, x, nF, ctx=ctx)
     assert np.all(En1[acc] < En0[acc])
     assert np.array_equal(np.asarray(E1.Tr)[~acc], np.asarray(E.Tr)[~acc])
+
+
+@pytest.mark.gpu
+def test_trained_network_gain_over_the_plain_method(ctx):
+    """What the shipped network gains: on the training script's validation
+    scans (seed 5001) its loss against the zero proposal, and at the coarsest
+    level the motion error with and without the proposal after 9 outer
+    iterations (the proposal may not make it worse)."""
+    import os
+    from disorder_b200 import proposal as pr
+    if not os.path.exists(pr.WEIGHTS):
+        pytest.skip("no trained weights")
+    net = pr.MotionNet.load(ctx, pr.WEIGHTS)
+    val = pr.make_dataset(ctx, 16, 5001)
+    loss, zero = pr.evaluate(net, val)
+    plain, learned = pr.compare(ctx, net, n_scans=2, n_outer=9)
+    print("validation loss %.4f (zero proposal %.4f)" % (loss, zero))
+    for a, b in zip(plain, learned):
+        print("final error plain %.3f vox %.3f deg, learned %.3f vox %.3f deg, %d proposals kept"
+              % (a["err_vox"][-1], a["err_deg"][-1], b["err_vox"][-1], b["err_deg"][-1], b["accepted"]))
+        assert b["err_vox"][-1] <= a["err_vox"][-1] + 0.25
+        assert b["err_deg"][-1] <= a["err_deg"][-1] + 0.5
+    assert loss < 0.95 * zero
