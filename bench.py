@@ -578,6 +578,14 @@ def main():
 
     Sh, _Sbuf = pinned(sc.S)
     yh, _ybuf = pinned(sc.y)
+    # one untimed pass of the same path first (as the device-timed steps have
+    # warm-up steps): the device pool then holds the memory of the uploaded
+    # inputs instead of growing inside the timed region
+    Sd = ctx.upload(Sh)
+    yd = ctx.upload(yh)
+    xe, _, _ = one(Sd, yd)
+    xe.numpy()
+    del Sd, yd, xe
     ctx.synchronize()
     t0 = time.perf_counter()
     eclk = NvmlClockSampler(local)
