@@ -355,14 +355,15 @@ def calibrate_gain(ctx, data, net_D=LEVEL_N):
     return 1.0 / float(np.median(r))
 
 
-def train(ctx, net, data, epochs, lr=1e-3, seed=0, log=None, lr_end=1e-4):
+def train(ctx, net, data, epochs, lr=1e-3, seed=0, log=None, lr_end=1e-4, it0=0, total=None):
     """Adam over the scans (one scan's shots per batch), cosine learning rate
-    from lr to lr_end. Returns the mean training loss of each epoch."""
+    from lr to lr_end over `total` steps (default: this call's), starting at
+    step it0. Returns (mean training loss of each epoch, next step)."""
     rng = np.random.default_rng(seed)
     grad = ctx.empty((net.P,), np.float32)
     hist = []
-    total = epochs * len(data)
-    it = 0
+    total = total if total is not None else epochs * len(data)
+    it = it0
     tg = [ctx.upload(np.ascontiguousarray(t).T.copy(order="F")) for _, _, _, t in data]
     for ep in range(epochs):
         losses = []
@@ -371,13 +372,13 @@ def train(ctx, net, data, epochs, lr=1e-3, seed=0, log=None, lr_end=1e-4):
             B = t.shape[0]
             net.forward(feats, x, B, sc * net.gain, sc)
             losses.append(net.backward(tg[j], B, grad))
-            f = it / max(total - 1, 1)
+            f = min(it / max(total - 1, 1), 1.0)
             net.adam(grad, lr_end + 0.5 * (lr - lr_end) * (1 + math.cos(math.pi * f)))
             it += 1
         hist.append(float(np.mean(losses)))
         if log:
             log("epoch %d loss %.4f" % (ep, hist[-1]))
-    return hist
+    return hist, it
 
 
 def evaluate(net, data):
@@ -392,31 +393,44 @@ def evaluate(net, data):
 
 def main():
     """Train the proposal network on simulated shots and write its weights:
-    python -m disorder_b200.proposal [--scans 320] [--epochs 12] [--out PATH]"""
+    python -m disorder_b200.proposal [--scans 320] [--rounds 1] [--epochs 16] [--out PATH]
+    Each round simulates --scans fresh scans and trains --epochs on them; one
+    cosine learning-rate schedule spans all rounds."""
     import argparse
     ap = argparse.ArgumentParser()
     ap.add_argument("--scans", type=int, default=320)
+    ap.add_argument("--rounds", type=int, default=1)
     ap.add_argument("--val", type=int, default=16)
-    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--epochs", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=5000)
     ap.add_argument("--out", default=WEIGHTS)
     a = ap.parse_args()
     ctx = api.Context(0)
-    t0 = time.time()
-    data = make_dataset(ctx, a.scans, a.seed)
     val = make_dataset(ctx, a.val, a.seed + 1)
-    t_gen = time.time() - t0
     net = MotionNet(ctx, LEVEL_N, 64, params=init_params(np.random.default_rng(a.seed)))
-    net.gain = calibrate_gain(ctx, data)
-    print("generated %d training shots in %.1f s, gain %.4g" % (a.scans * 64, t_gen, net.gain), flush=True)
-    t0 = time.time()
-    hist = train(ctx, net, data, a.epochs, a.lr, seed=a.seed, log=lambda s: print(s, flush=True))
-    t_train = time.time() - t0
-    vl, vz = evaluate(net, val)
-    print("trained in %.1f s; validation loss %.4f (zero proposal %.4f)" % (t_train, vl, vz), flush=True)
+    total = a.rounds * a.epochs * a.scans
+    it, hist, t_gen, t_train = 0, [], 0.0, 0.0
+    for r in range(a.rounds):
+        t0 = time.time()
+        data = make_dataset(ctx, a.scans, a.seed if r == 0 else a.seed + 7919 * r)
+        t_gen += time.time() - t0
+        if r == 0:
+            net.gain = calibrate_gain(ctx, data)
+        print("round %d: %d training shots, gain %.4g" % (r, a.scans * 64, net.gain), flush=True)
+        t0 = time.time()
+        h, it = train(ctx, net, data, a.epochs, a.lr, seed=a.seed + r, log=lambda s: print(s, flush=True),
+                      it0=it, total=total)
+        t_train += time.time() - t0
+        hist += h
+        vl, vz = evaluate(net, val)
+        print("round %d: validation loss %.4f (zero proposal %.4f)" % (r, vl, vz), flush=True)
+        del data
+    print("simulated %d shots in %.1f s, trained in %.1f s; validation loss %.4f (zero proposal %.4f)"
+          % (a.rounds * a.scans * 64, t_gen, t_train, vl, vz), flush=True)
     net.save(a.out, meta=dict(train_loss=np.array(hist), val_loss=np.float64(vl), val_zero=np.float64(vz),
-                              scans=np.int64(a.scans), epochs=np.int64(a.epochs), seed=np.int64(a.seed)))
+                              scans=np.int64(a.scans * a.rounds), epochs=np.int64(a.epochs),
+                              rounds=np.int64(a.rounds), seed=np.int64(a.seed)))
 
 
 if __name__ == "__main__":
