@@ -36,6 +36,20 @@ DIS_HD float2 csub(float2 a, float2 b) {
   return make_float2(a.x - b.x, a.y - b.y);
 #endif
 }
+// acc + a * s on both lanes: one packed fma.rn.f32x2 on sm_100, per lane the
+// same single rounding as fmaf.
+DIS_HD float2 cfmas(float2 a, float s, float2 acc) {
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000)
+  float2 r;
+  asm("{\n\t.reg .b64 pa, ps, pc, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 ps, {%4, %4};\n\t"
+      "mov.b64 pc, {%5, %6};\n\tfma.rn.f32x2 pd, pa, ps, pc;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(s), "f"(acc.x), "f"(acc.y));
+  return r;
+#else
+  return make_float2(fmaf(a.x, s, acc.x), fmaf(a.y, s, acc.y));
+#endif
+}
 DIS_HD float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 DIS_HD float2 cmulc(float2 a, float2 b) { return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }  // a*conj(b)
 DIS_HD float2 cconj(float2 a) { return make_float2(a.x, -a.y); }

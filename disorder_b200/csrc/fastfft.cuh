@@ -94,10 +94,8 @@ struct DFT {
 #pragma unroll
         for (int r = 1; r <= H; ++r) {
           const float2 w = root<R>((q * r) % R);  // (cos, -sin)
-          A.x = fmaf(a[r - 1].x, w.x, A.x);
-          A.y = fmaf(a[r - 1].y, w.x, A.y);
-          B.x = fmaf(b[r - 1].x, w.y, B.x);
-          B.y = fmaf(b[r - 1].y, w.y, B.y);
+          A = cfmas(a[r - 1], w.x, A);
+          B = cfmas(b[r - 1], w.y, B);
         }
         // forward: X_q = A + i B, X_{R-q} = A - i B (B carries -sin)
         const float2 iB = make_float2(-B.y, B.x);
