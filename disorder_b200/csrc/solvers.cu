@@ -372,6 +372,26 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   DIS_TRY(red_init(ctx, &rws, &R));
   std::vector<int> segs;
   for (int q = 0; q < plan->n_seg; ++q) segs.push_back(q);
+  // Tracking the residual from an initial guess: r = E x0 - y is needed
+  // anyway, and without EH.Mb (which decode applies and encodedecode does
+  // not) b - EHE(x0) = -constrain(decode(W r) + Ti x0). One decode of r then
+  // replaces the decode of y and the normal operator on x0 (:46, :53-56).
+  const bool fused_init = track && x_init && !s.Mb;
+  auto encode_residual = [&]() -> int {  // rbuf = E x - y
+    EncodeSpec sp;
+    sp.x = x;
+    sp.Sf = s.Sf;
+    sp.C = s.C;
+    sp.T = s.T;
+    sp.T_n = plan->n_mot;
+    sp.segs = all_segs;
+    sp.n3_lo = 0;
+    sp.N3c = plan->N[2];
+    sp.y_ld = plan->n_samples;
+    sp.y_n3off = 0;
+    sp.y_N3 = plan->N[2];
+    return dis_encode_segments(ctx, plan, sp, rbuf, s.y);
+  };
   // b = constrain(decode(y))   (:46)
   DecodeSpec ds;
   ds.y = s.y;
@@ -382,11 +402,18 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   ds.segs = segs;
   ds.We = s.We;
   ds.Mb = s.Mb;
-  DIS_TRY(dis_decode_segments(ctx, plan, ds, b));
   const int blocks = kRedBlocks;
-  if (s.C_Ma) {
-    constrain_kernel<<<blocks, 256, 0, ctx->stream>>>(b, s.C_Ma, V);
-    dis_count(ctx);
+  if (fused_init) {
+    DIS_TRY(encode_residual());
+    ds.y = rbuf;
+    DIS_TRY(dis_decode_segments(ctx, plan, ds, ehe));  // E^H W (E x0 - y)
+    DIS_CUDA_TRY(cudaMemsetAsync(b, 0, sizeof(float2) * V, ctx->stream));
+  } else {
+    DIS_TRY(dis_decode_segments(ctx, plan, ds, b));
+    if (s.C_Ma) {
+      constrain_kernel<<<blocks, 256, 0, ctx->stream>>>(b, s.C_Ma, V);
+      dis_count(ctx);
+    }
   }
   EncodeDecodeSpec es;
   es.x = nullptr;
@@ -405,7 +432,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   double dummy = 0;
   // EHE for the initial guess (:53-56)
   if (x_init) {
-    DIS_TRY(normal_op(x, ehe, nullptr));
+    if (!fused_init) DIS_TRY(normal_op(x, ehe, nullptr));
     pap_kernel<<<blocks, 256, 0, ctx->stream>>>(x, ehe, s.C_Ma, s.R_Ti, V, R.part);
     dis_count(ctx);
     DIS_TRY(red_finish(R, &dummy, nullptr));
@@ -428,19 +455,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   if (track) {
     // r = E x0 - y (x0 = 0: r = -y)
     if (x_init) {
-      EncodeSpec sp;
-      sp.x = x;
-      sp.Sf = s.Sf;
-      sp.C = s.C;
-      sp.T = s.T;
-      sp.T_n = plan->n_mot;
-      sp.segs = all_segs;
-      sp.n3_lo = 0;
-      sp.N3c = plan->N[2];
-      sp.y_ld = plan->n_samples;
-      sp.y_n3off = 0;
-      sp.y_N3 = plan->N[2];
-      DIS_TRY(dis_encode_segments(ctx, plan, sp, rbuf, s.y));
+      if (!fused_init) DIS_TRY(encode_residual());
     } else {
       neg_kernel<<<blocks, 256, 0, ctx->stream>>>(rbuf, s.y, ny);
       dis_count(ctx);

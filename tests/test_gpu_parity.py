@@ -219,9 +219,10 @@ def test_compute_energy(ctx):
 
 # (44, 44, 22) reaches the TMA weighted pass, which also emits the forward
 # samples that CG's Energy tolerance tracks; (16, 16, 12) the separate gather
-@pytest.mark.parametrize("tolType,nIt,N", [("RelativeResidual2Error", 4, (16, 16, 12)), ("Energy", 7, (16, 16, 12)),
-                                          ("Energy", 7, (44, 44, 22))])
-def test_cg(ctx, tolType, nIt, N):
+@pytest.mark.parametrize("tolType,nIt,N,we", [("RelativeResidual2Error", 4, (16, 16, 12), False),
+                                             ("Energy", 7, (16, 16, 12), False), ("Energy", 7, (44, 44, 22), False),
+                                             ("Energy", 5, (44, 44, 22), True)])
+def test_cg(ctx, tolType, nIt, N, we):
     import disorder_b200 as db
     from oracle import encoding as oenc
     from oracle import solvers as osol
@@ -230,10 +231,14 @@ def test_cg(ctx, tolType, nIt, N):
     Se = (1.0 / (np.sum(np.abs(sc.S) ** 2, axis=3) + 1e-9)).astype(np.float32)
     mbe = (np.arange(N[2]) >= 3).astype(np.float32)
     x0 = 0.5 * sc.x_gt
-    x, En, nn = db.CGsolver(y.astype(np.complex64), Ed, db.Struct(Mbe=mbe), db.Struct(Se=Se), None, None, x0, nIt,
+    # per-sample weights (EH.We, the outlier rejection's soft shot weights)
+    wsmp = np.random.default_rng(5).uniform(0.3, 1.0, y.shape[0]).astype(np.float32) if we else None
+    EHd = db.Struct(Mbe=mbe, We=wsmp) if we else db.Struct(Mbe=mbe)
+    EHo = (Eo.__class__(Mbe=mbe.astype(np.float64), We=wsmp.astype(np.float64)) if we
+           else Eo.__class__(Mbe=mbe.astype(np.float64)))
+    x, En, nn = db.CGsolver(y.astype(np.complex64), Ed, EHd, db.Struct(Se=Se), None, None, x0, nIt,
                             tolType, 0.0, ctx=ctx)
-    xo, Eno, nno = osol.CGsolver(y, Eo, Eo.__class__(Mbe=mbe.astype(np.float64)),
-                                 Eo.__class__(Se=Se.astype(np.float64)), None, None,
+    xo, Eno, nno = osol.CGsolver(y, Eo, EHo, Eo.__class__(Se=Se.astype(np.float64)), None, None,
                                  x0.astype(np.complex128), nIt, tolType, 0.0)
     assert nn == nno
     assert rel(x, xo) < TOL_SOLVER
