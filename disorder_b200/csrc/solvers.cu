@@ -331,7 +331,14 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   std::vector<int> all_segs;
   for (int q = 0; q < plan->n_seg; ++q) all_segs.push_back(q);
   const bool track = tolType == 6 && !dis_plane_usable(plan, s.C, all_segs);
-  const size_t need = sizeof(float2) * (5 * V + (tolType == 6 ? ny : 0) + (track ? ny : 0)) +
+  // From an initial guess x0, with r = E x0 - y and without EH.Mb (which
+  // decode applies and encodedecode does not), b - EHE(x0) =
+  // -constrain(decode(W r) + Ti x0): one encode and one decode replace the
+  // decode of y and the normal operator on x0 (:46, :53-56). b itself is
+  // needed only by the RelativeResidual2Error test with a positive tolerance.
+  const bool need_b = tolType == 1 && tol > 0;
+  const bool fused_init = x_init && !s.Mb && (track || !need_b);
+  const size_t need = sizeof(float2) * (5 * V + (tolType == 6 || fused_init ? ny : 0) + (track ? ny : 0)) +
                       sizeof(float) * (wm + plan->N[2]) + (1 << 20);
   Workspace ws;
   DIS_TRY(dis_workspace2(ctx, need, &ws));
@@ -342,9 +349,9 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   float2* ehe = ws.take<float2>(V);
   float* wmap = ws.take<float>(wm);
   float* roww = ws.take<float>(plan->N[2]);
-  float2* rbuf = tolType == 6 ? ws.take<float2>(ny) : nullptr;
+  float2* rbuf = tolType == 6 || fused_init ? ws.take<float2>(ny) : nullptr;
   float2* ebuf = track ? ws.take<float2>(ny) : nullptr;
-  if (!b || !r || !z || !p || !ehe || !wmap || !roww || (tolType == 6 && !rbuf) || (track && !ebuf))
+  if (!b || !r || !z || !p || !ehe || !wmap || !roww || ((tolType == 6 || fused_init) && !rbuf) || (track && !ebuf))
     return dis_set_error(ctx, DISORDER_OOM, "CG workspace");
   DIS_TRY(dis_build_weight_map(ctx, plan, s.We, wmap, 1.f));
   const bool haveRow = s.Mb || s.Mbe;
@@ -372,11 +379,6 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   DIS_TRY(red_init(ctx, &rws, &R));
   std::vector<int> segs;
   for (int q = 0; q < plan->n_seg; ++q) segs.push_back(q);
-  // Tracking the residual from an initial guess: r = E x0 - y is needed
-  // anyway, and without EH.Mb (which decode applies and encodedecode does
-  // not) b - EHE(x0) = -constrain(decode(W r) + Ti x0). One decode of r then
-  // replaces the decode of y and the normal operator on x0 (:46, :53-56).
-  const bool fused_init = track && x_init && !s.Mb;
   auto encode_residual = [&]() -> int {  // rbuf = E x - y
     EncodeSpec sp;
     sp.x = x;
@@ -440,7 +442,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
     DIS_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(float2) * V, ctx->stream));
   }
   double bnorm2 = 1.0;
-  if (tolType != 6 && tolType != 7) {  // :58-62
+  if (tolType != 6 && tolType != 7 && !fused_init) {  // :58-62 (unused when the tolerance is not positive)
     wnorm_kernel<<<blocks, 256, 0, ctx->stream>>>(b, s.P_Se, V, R.part);
     dis_count(ctx);
     DIS_TRY(red_finish(R, &bnorm2, nullptr));

@@ -219,10 +219,14 @@ def test_compute_energy(ctx):
 
 # (44, 44, 22) reaches the TMA weighted pass, which also emits the forward
 # samples that CG's Energy tolerance tracks; (16, 16, 12) the separate gather
-@pytest.mark.parametrize("tolType,nIt,N,we", [("RelativeResidual2Error", 4, (16, 16, 12), False),
-                                             ("Energy", 7, (16, 16, 12), False), ("Energy", 7, (44, 44, 22), False),
-                                             ("Energy", 5, (44, 44, 22), True)])
-def test_cg(ctx, tolType, nIt, N, we):
+# tol 0 with an initial guess starts from one encode and one decode of the
+# residual; a positive RelativeResidual2Error tolerance needs b = decode(y)
+@pytest.mark.parametrize("tolType,nIt,N,we,tol", [("RelativeResidual2Error", 4, (16, 16, 12), False, 0.0),
+                                                 ("RelativeResidual2Error", 4, (44, 44, 22), False, 1e-12),
+                                                 ("Energy", 7, (16, 16, 12), False, 0.0),
+                                                 ("Energy", 7, (44, 44, 22), False, 0.0),
+                                                 ("Energy", 5, (44, 44, 22), True, 0.0)])
+def test_cg(ctx, tolType, nIt, N, we, tol):
     import disorder_b200 as db
     from oracle import encoding as oenc
     from oracle import solvers as osol
@@ -237,9 +241,9 @@ def test_cg(ctx, tolType, nIt, N, we):
     EHo = (Eo.__class__(Mbe=mbe.astype(np.float64), We=wsmp.astype(np.float64)) if we
            else Eo.__class__(Mbe=mbe.astype(np.float64)))
     x, En, nn = db.CGsolver(y.astype(np.complex64), Ed, EHd, db.Struct(Se=Se), None, None, x0, nIt,
-                            tolType, 0.0, ctx=ctx)
+                            tolType, tol, ctx=ctx)
     xo, Eno, nno = osol.CGsolver(y, Eo, EHo, Eo.__class__(Se=Se.astype(np.float64)), None, None,
-                                 x0.astype(np.complex128), nIt, tolType, 0.0)
+                                 x0.astype(np.complex128), nIt, tolType, tol)
     assert nn == nno
     assert rel(x, xo) < TOL_SOLVER
     if tolType == "Energy":
