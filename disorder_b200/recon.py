@@ -7,8 +7,8 @@ then outer iterations of CGsolver (:431) and LMsolver (:507) with the
 reference's motion-convergence resets (:379-388) and, once the motion has
 converged or at the last level, a final CGsolver to the energy tolerance
 (:414-425, nIt=300, 'Energy', tolerSolve). Before every image update the
-motion states are binned by compressMotion (:392); the final image update
-weights the shots by the outlier rejection of the last motion level
+motion states are binned by compressMotion (:392); from the levels with
+leff >= 0 on, the image updates weight the shots by the outlier rejection
 (:440-482). NIfTI output, the CS/shearlet reconstruction and the
 Gibbs/B-spline filters of the reference driver are not part of this path.
 """
@@ -176,6 +176,14 @@ def outlier_weights(Re, sweeps, n_sweeps, leff, percRobustShot=(0.125, 0.25), en
     return np.minimum(tail / ((1.0 - enerRobustShot) / n_sweeps), 1.0)
 
 
+def _sample_weights(We_shot, mSt, n_states):
+    """Per-sample EH.We from shot weights; outer samples keep 1 (solveXT.m:480-481)."""
+    w = np.ones(len(mSt), np.float32)
+    inner = np.asarray(mSt) < n_states
+    w[inner] = np.asarray(We_shot)[np.asarray(mSt)[inner]]
+    return w
+
+
 class ReconLog:
     def __init__(self):
         self.events = []
@@ -201,9 +209,9 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
     step from there (no counterpart in the reference). levels: run only
     the first levels of the pyramid. traLimX: motion binning limits of the
     image update (compressMotion; None: no binning). outliers: the shot
-    weights of the outlier rejection (rec.Alg.AlignedRec=2, solveXT.m:440-482)
-    from the last motion level at full in-plane sampling, applied in the final
-    image update. Returns (x device volume, T (n_states, 6), log).
+    weights of the outlier rejection (rec.Alg.AlignedRec=2, solveXT.m:440-482),
+    computed after each image update at the levels with leff >= 0 and applied
+    to the later image updates of that level and to the final one. Returns (x device volume, T (n_states, 6), log).
     """
     log = log if log is not None else ReconLog()
     N = tuple(int(n) for n in N)
@@ -246,10 +254,7 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
         EH = api.Struct(Mbe=Mbe_d)
         if not estT[l] and leff > 0 and We_shot is not None and np.any(We_shot < 1):
             # soft shot weights in the final image update (solveXT.m:411-415)
-            wsmp = np.ones(len(mSt), np.float32)
-            inner = mSt < n_states
-            wsmp[inner] = We_shot[mSt[inner]]
-            EH = api.Struct(Mbe=Mbe_d, We=wsmp)
+            EH = api.Struct(Mbe=Mbe_d, We=_sample_weights(We_shot, mSt, n_states))
         A = api.Struct(Se=Se)
         est = bool(estT[l])
         use_net = proposal is not None and est and tuple(NXres) == tuple(proposal.D)
@@ -274,6 +279,9 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
                 Re = api.sampleEnergies(yRes, xRes, Ex, EH, ctx=ctx)
                 We_shot = outlier_weights(Re, mSt, n_states, leff)
                 log.add(step="outliers", level=l, it=n, rejected=int(np.sum(We_shot < 1)))
+                # soft shot weights for the next image updates of this level (:478-482)
+                EH = api.Struct(Mbe=Mbe_d, We=_sample_weights(We_shot, mSt, n_states)) if np.any(We_shot < 1) \
+                    else api.Struct(Mbe=Mbe_d)
             if use_net:
                 # a proposal that lowers a state's energy moves that state's
                 # motion; the LM step then runs from there for every state
