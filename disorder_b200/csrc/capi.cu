@@ -108,6 +108,18 @@ int disorder_ctx_create(int device, disorder_ctx* out) {
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    // DISORDER_POOL_RESERVE_GB: grow the pool once, now, by allocating and
+    // freeing that much, so that later allocations of varying sizes are
+    // carved from memory it holds instead of mapping more in mid-run
+    const char* e = std::getenv("DISORDER_POOL_RESERVE_GB");
+    const double gb = e ? std::atof(e) : 0.0;
+    if (use_pool() && gb > 0) {
+      void* p = nullptr;
+      if (cudaMallocAsync(&p, (size_t)(gb * (1ull << 30)), ctx->stream) == cudaSuccess) {
+        cudaFreeAsync(p, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+      }
+    }
   }
   cudaGetLastError();
   if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess || cudaMemset(ctx->d_err, 0, 256) != cudaSuccess) {
