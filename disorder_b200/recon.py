@@ -226,7 +226,8 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
     E = None
     n_coarse = int(np.sum(resPyr != 1))
     We_shot = None
-    for l in range(L if levels is None else min(L, levels)):
+    n_run = L if levels is None else min(L, levels)
+    for l in range(n_run):
         leff = l + 1 - n_coarse  # solveXT.m:269
         NXres = tuple(int(math.ceil(n * resPyr[l])) for n in N)
         # level operators (downsampleOperators, solveXT.m:333-342)
@@ -272,16 +273,18 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
             Ex = binned(E, resIso[-1], traLimX) if traLimX is not None else E  # solveXT.m:392
             xRes, EnX, nn = api.CGsolver(yRes, Ex, EH, A, None, None, xRes, nX, tolType, tol, ctx=ctx)
             log.add(step="cg", level=l, it=n, iters=nn, tolType=tolType, states=int(Ex.NMs))
-            if not est:
-                break
-            if outliers and leff >= 0:
-                # residual energy per sample and outlier detection (solveXT.m:440-466)
+            if outliers and leff >= 0 and l < n_run - 1:
+                # residual energy per sample and outlier detection after every
+                # image update, the level's last one included (solveXT.m:440-466);
+                # the final level's weights are not used again
                 Re = api.sampleEnergies(yRes, xRes, Ex, EH, ctx=ctx)
                 We_shot = outlier_weights(Re, mSt, n_states, leff)
                 log.add(step="outliers", level=l, it=n, rejected=int(np.sum(We_shot < 1)))
                 # soft shot weights for the next image updates of this level (:478-482)
                 EH = api.Struct(Mbe=Mbe_d, We=_sample_weights(We_shot, mSt, n_states)) if np.any(We_shot < 1) \
                     else api.Struct(Mbe=Mbe_d)
+            if not est:
+                break
             if use_net:
                 # a proposal that lowers a state's energy moves that state's
                 # motion; the LM step then runs from there for every state
