@@ -52,6 +52,8 @@ SIGNATURES = [
     ("disorder_memcpy_d2h", C.c_int, [VP, VP, VP, C.c_size_t]),
     ("disorder_memcpy_d2d", C.c_int, [VP, VP, VP, C.c_size_t]),
     ("disorder_memset", C.c_int, [VP, VP, C.c_int, C.c_size_t]),
+    ("disorder_upload", C.c_int, [VP, VP, C.c_size_t, C.POINTER(VP)]),
+    ("disorder_download", C.c_int, [VP, VP, VP, C.c_size_t]),
     ("disorder_kernel_launches", C.c_int64, [VP]),
     ("disorder_event_record", C.c_int, [VP, I32]),
     ("disorder_event_elapsed", C.c_int, [VP, I32, I32, FP]),
@@ -59,6 +61,7 @@ SIGNATURES = [
     ("disorder_plan_destroy", C.c_int, [VP]),
     ("disorder_sinc_rigid_transform", C.c_int, [VP, VP, VP, I32, FP, I32, I32, I32, I32, VP]),
     ("disorder_sinc_rigid_transform_static", C.c_int, [VP, VP, VP, I32, FP, I32, I32, I32, VP]),
+    ("disorder_precompute_factors", C.c_int, [VP, VP, FP, I32, I32, VP, VP, VP, C.POINTER(C.c_uint8)]),
     ("disorder_sinc_rigid_transform_gradient", C.c_int, [VP, VP, VP, FP, I32, VP, VP]),
     ("disorder_encode", C.c_int, [VP, VP, VP, VP, I32, FP, VP]),
     ("disorder_decode", C.c_int, [VP, VP, VP, VP, I32, FP, VP, VP, VP]),

@@ -468,6 +468,37 @@ class Factors:
     def __init__(self, grids, T, di, cg):
         self.grids, self.T, self.di, self.cg = grids, np.asarray(T, np.float32), di, cg
 
+    def arrays(self, ctx=None):
+        """The factors as the reference holds them (disorder_precompute_factors):
+        {'e1': [N[m] x S], 'e2': [N[a] x N[b] x S], 'e3': [...], 'flip': (3, S)}
+        with (a, b) = (0, 1), (0, 2), (1, 2) for m = 0, 1, 2."""
+        ctx = ctx or default_context()
+        p = _transform_plan(ctx, self.grids)
+        N = tuple(int(n) for n in p.N)
+        S = int(self.T.shape[0])
+        pairs = [(0, 1), (0, 2), (1, 2)]
+        n2 = sum(N[a] * N[b] for a, b in pairs) * S
+        e1 = ctx.empty((sum(N) * S,))
+        e2 = ctx.empty((n2,))
+        e3 = ctx.empty((n2,))
+        flip = np.zeros(3 * S, np.uint8)
+        Tf = np.asfortranarray(self.T)
+        ctx.check(ctx.lib.disorder_precompute_factors(ctx.h, p.h, Tf.ctypes.data_as(_lib.FP), S, int(self.di), e1.ptr,
+                                                      e2.ptr, e3.ptr, flip.ctypes.data_as(C.POINTER(C.c_uint8))))
+        h1, h2, h3 = e1.numpy(), e2.numpy(), e3.numpy()
+        out = {"e1": [], "e2": [], "e3": [], "flip": flip.reshape(3, S).astype(bool)}
+        o = 0
+        for m in range(3):
+            out["e1"].append(h1[o:o + N[m] * S].reshape((N[m], S), order="F"))
+            o += N[m] * S
+        o = 0
+        for a, b in pairs:
+            n = N[a] * N[b] * S
+            out["e2"].append(h2[o:o + n].reshape((N[a], N[b], S), order="F"))
+            out["e3"].append(h3[o:o + n].reshape((N[a], N[b], S), order="F"))
+            o += n
+        return out
+
 
 def precomputeFactorsSincRigidTransform(grids, T, di=1, cg=0):
     """Methods/precomputeFactorsSincRigidTransform.m:1 with gr=1, sh=1.

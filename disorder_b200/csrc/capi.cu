@@ -225,6 +225,28 @@ int disorder_memcpy_d2h(disorder_ctx ctx, void* dst, const void* src, size_t byt
   return DISORDER_OK;
 }
 
+int disorder_upload(disorder_ctx ctx, const void* host, size_t bytes, void** dptr) {
+  CTX_CHECK(ctx);
+  if (!dptr || (!host && bytes)) return dis_set_error(ctx, DISORDER_BAD_ARG, "upload: null argument");
+  *dptr = nullptr;
+  void* d = nullptr;
+  DIS_TRY(disorder_malloc(ctx, bytes, &d));
+  const int st = bytes ? disorder_memcpy_h2d(ctx, d, host, bytes) : DISORDER_OK;
+  if (st != DISORDER_OK) {
+    disorder_free(ctx, d);
+    return st;
+  }
+  *dptr = d;
+  return DISORDER_OK;
+}
+
+int disorder_download(disorder_ctx ctx, const void* dptr, void* host, size_t bytes) {
+  CTX_CHECK(ctx);
+  if (!bytes) return DISORDER_OK;
+  if (!dptr || !host) return dis_set_error(ctx, DISORDER_BAD_ARG, "download: null argument");
+  return disorder_memcpy_d2h(ctx, host, dptr, bytes);
+}
+
 int disorder_memcpy_d2d(disorder_ctx ctx, void* dst, const void* src, size_t bytes) {
   CTX_CHECK(ctx);
   DEV_GUARD(ctx);

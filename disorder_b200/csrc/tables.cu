@@ -4,6 +4,7 @@
 // double precision; the per-element factors exp(i*phase) are evaluated on the
 // device in double precision and rounded to single. The 1/N of the inverse
 // DFT of the pass that applies a factor is folded into that factor.
+#include <algorithm>
 #include <cmath>
 
 #include "fastpass.h"
@@ -313,5 +314,98 @@ int dis_build_tables(disorder_ctx_s* ctx, const disorder_plan_s* plan, const std
   // (pageable-source async copies are staged before they return, so the
   // host vectors above may go out of scope)
   DIS_CUDA_TRY(cudaGetLastError());
+  return DISORDER_OK;
+}
+
+// ---------------------------------------------------------------- factors as arrays
+namespace {
+
+// out[(i + Nlo*j) + Nlo*Nhi*s] = exp(i * coef[s] * rk), rk the single-precision
+// product rG[ra][.] * kG[ka][.] over the two dims lo < hi of {ra, ka}
+__global__ void shear_factor_kernel(const float* __restrict__ rG, const float* __restrict__ kG, int Nlo, int Nhi,
+                                    int r_is_lo, const double* __restrict__ coef, int S, float2* __restrict__ out) {
+  const long long n = (long long)Nlo * Nhi * S;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % Nlo);
+    const long long q = e / Nlo;
+    const int j = (int)(q % Nhi);
+    const int s = (int)(q / Nhi);
+    const float rk = r_is_lo ? rG[i] * kG[j] : rG[j] * kG[i];
+    double sn, cs;
+    sincos(coef[s] * (double)rk, &sn, &cs);
+    out[e] = make_float2((float)cs, (float)sn);
+  }
+}
+
+// out[k + N*s] = exp(i * t[s] * kG[k])
+__global__ void ramp_factor_kernel(const float* __restrict__ kG, int N, const double* __restrict__ t, int S,
+                                   float2* __restrict__ out) {
+  const long long n = (long long)N * S;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(e % N);
+    const int s = (int)(e / N);
+    double sn, cs;
+    sincos(t[s] * (double)kG[k], &sn, &cs);
+    out[e] = make_float2((float)cs, (float)sn);
+  }
+}
+
+}  // namespace
+
+extern "C" int disorder_precompute_factors(disorder_ctx ctx, disorder_plan plan, const float* T, int32_t n_states,
+                                           int32_t di, void* e1, void* e2, void* e3, uint8_t* flip) {
+  if (!ctx) return DISORDER_BAD_ARG;
+  if (!plan || plan->ctx != ctx) return dis_set_error(ctx, DISORDER_BAD_ARG, "bad plan");
+  if (!T || n_states < 1 || (di != 0 && di != 1))
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "precompute factors: bad arguments");
+  DIS_CUDA_TRY(cudaSetDevice(ctx->device));
+  const int S = n_states;
+  std::vector<SlotParams> prm;
+  dis_slot_params(T, S, nullptr, S, di, &prm);
+  if (flip)
+    for (int m = 0; m < 3; ++m)
+      for (int s = 0; s < S; ++s) flip[m * S + s] = (uint8_t)prm[s].flip[m];
+  // per-state coefficients: t (e1), tau (e2), sig (e3) for the 3 blocks
+  std::vector<double> h((size_t)9 * S);
+  for (int m = 0; m < 3; ++m)
+    for (int s = 0; s < S; ++s) {
+      h[(size_t)(0 * 3 + m) * S + s] = prm[s].t[m];
+      h[(size_t)(1 * 3 + m) * S + s] = prm[s].tau[m];
+      h[(size_t)(2 * 3 + m) * S + s] = prm[s].sig[m];
+    }
+  Workspace ws;
+  DIS_TRY(dis_small(ctx, &ws));
+  double* d = ws.take<double>(h.size());
+  if (!d) return dis_set_error(ctx, DISORDER_OOM, "precompute factors: scratch");
+  DIS_CUDA_TRY(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  const int* N = plan->N;
+  // rkGrid{1}{m}: rG along per(2,m), kG along per(1,m); rkGrid{2}{m} the
+  // reverse (Methods/generateTransformGrids.m:57-62, per = [1 3 2; 2 1 3])
+  const int per[2][3] = {{0, 2, 1}, {1, 0, 2}};
+  long long off2 = 0;
+  long long off1 = 0;
+  for (int m = 0; m < 3; ++m) {
+    if (e1) {
+      ramp_factor_kernel<<<256, 256, 0, ctx->stream>>>(plan->d_kG[m], N[m], d + (size_t)m * S, S,
+                                                       (float2*)e1 + off1);
+      dis_count(ctx);
+    }
+    off1 += (long long)N[m] * S;
+    for (int which = 0; which < 2; ++which) {
+      void* out = which == 0 ? e2 : e3;
+      if (!out) continue;
+      const int ra = which == 0 ? per[1][m] : per[0][m];
+      const int ka = which == 0 ? per[0][m] : per[1][m];
+      const int lo = std::min(ra, ka), hi = std::max(ra, ka);
+      shear_factor_kernel<<<256, 256, 0, ctx->stream>>>(plan->d_rG[ra], plan->d_kG[ka], N[lo], N[hi], ra == lo ? 1 : 0,
+                                                        d + (size_t)((1 + which) * 3 + m) * S, S,
+                                                        (float2*)out + off2);
+      dis_count(ctx);
+    }
+    const int a = m == 2 ? 1 : 0, b = m == 0 ? 1 : 2;  // blocks span dims {0,1}, {0,2}, {1,2}
+    off2 += (long long)N[a] * N[b] * S;
+  }
+  DIS_CUDA_TRY(cudaGetLastError());
+  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return DISORDER_OK;
 }

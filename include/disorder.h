@@ -61,6 +61,12 @@ int disorder_free(disorder_ctx ctx, void* dptr);
 int disorder_memcpy_h2d(disorder_ctx ctx, void* dst, const void* src, size_t bytes);
 int disorder_memcpy_d2h(disorder_ctx ctx, void* dst, const void* src, size_t bytes);
 int disorder_memcpy_d2d(disorder_ctx ctx, void* dst, const void* src, size_t bytes);
+/* The MEX gateway's 'upload' / gather pair: disorder_upload allocates bytes
+ * (as disorder_malloc) and copies host data there, returning the device
+ * pointer that stays resident behind a handle; disorder_download copies it
+ * back to host memory. Free with disorder_free. */
+int disorder_upload(disorder_ctx ctx, const void* host, size_t bytes, void** dptr);
+int disorder_download(disorder_ctx ctx, const void* dptr, void* host, size_t bytes);
 int disorder_memset(disorder_ctx ctx, void* dst, int value, size_t bytes);
 /* number of kernels this context has launched since creation */
 int64_t disorder_kernel_launches(disorder_ctx ctx);
@@ -105,6 +111,25 @@ int disorder_plan_destroy(disorder_plan plan);
 int disorder_sinc_rigid_transform(disorder_ctx ctx, disorder_plan plan, const void* x,
                                   int32_t x_states, const float* T, int32_t n_states,
                                   int32_t di, int32_t sumR, int32_t useFull, void* out);
+
+/* et=precomputeFactorsSincRigidTransform(kG,rkG,T,di,0,1,1)
+ * (Methods/precomputeFactorsSincRigidTransform.m:24-133, gr=1, sh=1) as device
+ * arrays. The transforms above build these factors on the fly; this entry
+ * point materialises them for callers that want the reference's et.
+ * T: host n_states x 6. di: 1 forward, 0 inverse.
+ * e1: 3 consecutive blocks, block m is N[m] x n_states: et{1}{m} =
+ *     exp(i (-1)^di T(m) kGrid{m}) along dim m.
+ * e2, e3: 3 consecutive blocks each, block m is N[a] x N[b] x n_states over
+ *     the dims (a, b) = (1,2), (1,3), (2,3) for m = 1, 2, 3 that rkGrid{1}{m}
+ *     and rkGrid{2}{m} span: et{2}{m} = exp((-1)^(di-1) i tan(theta_m/2)
+ *     rkGrid{1}{m}) and et{3}{m} = exp((-1)^di i sin(theta_m) rkGrid{2}{m}),
+ *     theta wrapped to +-pi/2 after the flip test (rkGrid in single precision,
+ *     as the reference rounds it).
+ * flip: host 3 x n_states, flip[m*n_states + s] = |theta_m| > pi/2 (et{5}{m}).
+ * Any of e1, e2, e3, flip may be NULL. */
+int disorder_precompute_factors(disorder_ctx ctx, disorder_plan plan, const float* T,
+                                int32_t n_states, int32_t di, void* e1, void* e2, void* e3,
+                                uint8_t* flip);
 
 /* The sinc rigid transform above for callers that cannot let a library
  * allocate device memory (an application that reserves its whole device

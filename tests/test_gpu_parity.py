@@ -60,6 +60,38 @@ def _motion(rng, S, rot=5.0, tr=3.0):
     return T
 
 
+@pytest.mark.parametrize("di", [1, 0])
+def test_precompute_factors(ctx, di):
+    """et of precomputeFactorsSincRigidTransform as device arrays, against the
+    oracle (rotations beyond 90 degrees for the flip flags)."""
+    import disorder_b200 as db
+    from oracle.transform import precomputeFactorsSincRigidTransform as opf
+    N = (24, 20, 16)
+    rng = np.random.default_rng(41)
+    T = _motion(rng, 5)
+    T[1, 3] = np.radians(120.0)
+    T[3, 5] = np.radians(-100.0)
+    et, _ = db.precomputeFactorsSincRigidTransform(_grids(N), T, di)
+    got = et.arrays(ctx)
+    ref, _ = opf(_ogrids(N), T, di, 0)
+    for m in range(3):
+        assert np.array_equal(got["flip"][m], ref.flip[m])
+        assert rel(got["e1"][m], np.squeeze(ref.e1[m])) < TOL
+        assert rel(got["e2"][m], np.squeeze(ref.e2[m])) < TOL
+        assert rel(got["e3"][m], np.squeeze(ref.e3[m])) < TOL
+
+
+def test_upload_download_round_trip(ctx):
+    import ctypes as C
+    a = np.random.default_rng(2).standard_normal(1000).astype(np.float32)
+    d = C.c_void_p()
+    ctx.check(ctx.lib.disorder_upload(ctx.h, a.ctypes.data, a.nbytes, C.byref(d)))
+    b = np.zeros_like(a)
+    ctx.check(ctx.lib.disorder_download(ctx.h, d, b.ctypes.data, b.nbytes))
+    ctx.check(ctx.lib.disorder_free(ctx.h, d))
+    assert np.array_equal(a, b)
+
+
 GRID_SIZES = [(16, 12, 10), (32, 32, 24), (44, 40, 30), (96, 20, 12), (20, 160, 8), (64, 64, 44)]
 
 
