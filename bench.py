@@ -30,10 +30,6 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-# grow the library's device pool once, when the context is created, instead of
-# mid-run: allocations of varying sizes otherwise map new memory at random
-# points of some reconstructions (0.3-0.5 s each time)
-os.environ.setdefault("DISORDER_POOL_RESERVE_GB", "80")
 
 METRIC = "s per 3D aligned recon to plain-method NRMSE: learned+mixed vs plain, 1 B200"
 CFG = dict(N=(256, 256, 176), coils=32, coils_kept=16, shots=64, rot_deg=5.0, trans_vox=5.0, snr_db=25.0,
@@ -492,6 +488,10 @@ def main():
                     help="only time encode / decode / encodedecode of the scan size with SHOTS shots")
     ap.add_argument("--no-learned", action="store_true", help="skip the reconstruction with the learned proposal")
     args = ap.parse_args()
+    # grow the library's device pool once, when the context is created, instead
+    # of mid-run: allocations of varying sizes otherwise map new memory at
+    # random points of some reconstructions (0.3-0.5 s each time)
+    os.environ.setdefault("DISORDER_POOL_RESERVE_GB", "80")
     cfg = SMALL if args.small else CFG
     if args.transform_only:
         return transform_only(cfg, args.transform_only, args.warmup, args.steps)
