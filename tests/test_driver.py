@@ -132,3 +132,9 @@ def test_sample_energies_match_oracle():
     ref = oe.computeEnergy(y.astype(np.complex128), x.astype(np.complex128), Eo, EH=OStruct(Mb=Mb, Mbe=Mbe),
                            per_sample=True)
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
+
+
+def test_shot_weights_map_to_samples_and_outer_samples_keep_one():
+    mSt = np.array([0, 0, 1, 2, 2, 3, 3], np.int32)  # 3 shots, then the outer segment
+    w = recon._sample_weights(np.array([1.0, 0.25, 0.5]), mSt, 3)
+    assert w.dtype == np.float32 and list(w) == [1.0, 1.0, 0.25, 0.5, 0.5, 1.0, 1.0]
