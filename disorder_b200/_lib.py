@@ -69,6 +69,8 @@ SIGNATURES = [
     ("disorder_compute_energy", C.c_int, [VP, VP, VP, VP, VP, I32, FP, VP, VP, VP, DP]),
     ("disorder_cg_solve", C.c_int, [VP, VP, VP, VP, I32, FP, VP, VP, VP, VP, VP, VP, VP, I32, I32, I32, C.c_double,
                                     DP, C.POINTER(I32), C.POINTER(I32)]),
+    ("disorder_cg_solve_residual", C.c_int, [VP, VP, VP, VP, I32, FP, VP, VP, VP, VP, VP, VP, VP, I32, I32, I32,
+                                             C.c_double, DP, C.POINTER(I32), C.POINTER(I32), VP]),
     ("disorder_lm_step", C.c_int, [VP, VP, VP, VP, I32, VP, FP, FP, C.POINTER(C.c_uint8), C.c_float, FP, I32, I32,
                                    DP, DP]),
     ("disorder_resample", C.c_int, [VP, VP, C.POINTER(I32), I32, C.POINTER(I32), VP]),
@@ -78,6 +80,7 @@ SIGNATURES = [
                                           C.POINTER(I32), DP, DP]),
     ("disorder_state_energies", C.c_int, [VP, VP, VP, VP, I32, VP, FP, I32, I32, DP]),
     ("disorder_sample_energies", C.c_int, [VP, VP, VP, VP, I32, VP, FP, VP, DP]),
+    ("disorder_residual_energies", C.c_int, [VP, VP, VP, I32, VP, DP]),
     ("disorder_backproject_states", C.c_int, [VP, VP, VP, VP, I32, VP, FP, I32, I32, VP]),
     ("disorder_net_param_count", C.c_int64, []),
     ("disorder_net_create", C.c_int, [VP, C.POINTER(I32), I32, C.POINTER(VP)]),

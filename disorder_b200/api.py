@@ -382,11 +382,31 @@ def sampleEnergies(y, x, E, EH=None, ctx=None):
     return En[:p.n_samples]
 
 
+def residualSampleEnergies(r, E, EH=None, ctx=None):
+    """sampleEnergies for a residual r = encode(x) - y already on the device
+    (for example CGsolver's residual output). Returns (n_samples,) float64."""
+    ctx = ctx or default_context()
+    p = _plan(E, ctx)
+    Sd, _ = _dev(ctx, E.Sf, np.complex64)
+    Cn = Sd.shape[3] if len(Sd.shape) > 3 else 1
+    ws = [getattr(EH, f) for f in ("Mb", "Mbe") if EH is not None and EH.has(f)]
+    if len(ws) == 2:
+        ws = [np.prod([w.numpy() if isinstance(w, DeviceArray) else np.asarray(w) for w in ws], axis=0)]
+    Mbe, _ = _dev(ctx, ws[0] if ws else None, np.float32)
+    En = np.zeros(max(p.n_samples, 1))
+    ctx.check(ctx.lib.disorder_residual_energies(ctx.h, p.h, r.ptr, Cn, Mbe.ptr if Mbe else None,
+                                                 En.ctypes.data_as(_lib.DP)))
+    return En[:p.n_samples]
+
+
 TOLTYPES = {"RelativeResidual2Error": 1, "Energy": 6, "None": 7}
 
 
-def CGsolver(y, E, EH, A=None, Cs=None, R=None, x=None, nIt=300, tolType="Energy", tol=1e-5, ctx=None):
-    """Reconstruction/CGsolver.m:1-119 with E.Je=1. Returns (x, En, nn)."""
+def CGsolver(y, E, EH, A=None, Cs=None, R=None, x=None, nIt=300, tolType="Energy", tol=1e-5, ctx=None,
+             residual=None):
+    """Reconstruction/CGsolver.m:1-119 with E.Je=1. Returns (x, En, nn).
+    residual: optional device array (Ns, N3, C) that receives the final
+    sample residual encode(x) - y (disorder_cg_solve_residual)."""
     ctx = ctx or default_context()
     _check_fields(EH, EH_FIELDS, "EH")
     if tolType not in TOLTYPES:
@@ -413,9 +433,12 @@ def CGsolver(y, E, EH, A=None, Cs=None, R=None, x=None, nIt=300, tolType="Energy
     n_en, nn = C.c_int32(), C.c_int32()
     T = _T(E)
     ptr = lambda d: d.ptr if d is not None else None  # noqa: E731
-    ctx.check(ctx.lib.disorder_cg_solve(ctx.h, p.h, yd.ptr, Sd.ptr, Cn, T[1] if T else None, ptr(We), ptr(Mb),
-                                        ptr(Mbe), ptr(Se), ptr(Ma), ptr(Ti), xd.ptr, x_init, int(nIt),
-                                        TOLTYPES[tolType], float(tol), En, C.byref(n_en), C.byref(nn)))
+    args = (ctx.h, p.h, yd.ptr, Sd.ptr, Cn, T[1] if T else None, ptr(We), ptr(Mb), ptr(Mbe), ptr(Se), ptr(Ma),
+            ptr(Ti), xd.ptr, x_init, int(nIt), TOLTYPES[tolType], float(tol), En, C.byref(n_en), C.byref(nn))
+    if residual is not None:
+        ctx.check(ctx.lib.disorder_cg_solve_residual(*args, residual.ptr))
+    else:
+        ctx.check(ctx.lib.disorder_cg_solve(*args))
     Enm = np.array(En[:2 * n_en.value]).reshape(2, -1, order="F") if n_en.value else np.zeros((2, 0))
     return (_out(xd, host), Enm, nn.value)
 

@@ -574,6 +574,32 @@ int disorder_cg_solve(disorder_ctx ctx, disorder_plan plan, const void* y, const
   return st;
 }
 
+int disorder_cg_solve_residual(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf, int32_t n_coils,
+                               const float* T, const float* We, const float* Mb, const float* Mbe, const float* P_Se,
+                               const float* C_Ma, const float* R_Ti, void* x_inout, int32_t x_init, int32_t nIt,
+                               int32_t tolType, double tol, double* En, int32_t* n_en, int32_t* nn, void* r_out) {
+  PLAN_CHECK(ctx, plan);
+  if (!y || !Sf || !x_inout || n_coils < 1 || nIt < 0 || !n_en || !nn || !r_out)
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "cg_solve_residual: bad arguments");
+  CGSpec s;
+  s.y = (const float2*)y;
+  s.Sf = (const float2*)Sf;
+  s.C = n_coils;
+  s.T = T;
+  s.We = We;
+  s.Mb = Mb;
+  s.Mbe = Mbe;
+  s.P_Se = P_Se;
+  s.C_Ma = C_Ma;
+  s.R_Ti = R_Ti;
+  s.r_out = (float2*)r_out;
+  int a = 0, b = 0;
+  const int st = dis_cg_solve(ctx, plan, s, (float2*)x_inout, x_init, nIt, tolType, tol, En, &a, &b);
+  *n_en = a;
+  *nn = b;
+  return st;
+}
+
 int disorder_lm_step(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf, int32_t n_coils,
                      const void* x, float* T, float* w, uint8_t* cT, float winit, const float* tL, int32_t n3_lo,
                      int32_t n3_hi, double* En, double* EnPrev) {

@@ -793,6 +793,18 @@ int disorder_state_energies(disorder_ctx ctx, disorder_plan plan, const void* y,
   return DISORDER_OK;
 }
 
+// per-sample weighted residual energies of r into the host array En (d_en: device scratch)
+static int sample_energies_of(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* r, int C,
+                              const float* wrow, double* d_en, double* En) {
+  const long long ns = plan->n_samples;
+  sample_energy_kernel<<<blocks(ns), 256, 0, ctx->stream>>>(r, ns, plan->N[2], C, wrow, d_en);
+  dis_count(ctx);
+  DIS_CUDA_TRY(cudaGetLastError());
+  DIS_CUDA_TRY(cudaMemcpyAsync(En, d_en, sizeof(double) * ns, cudaMemcpyDeviceToHost, ctx->stream));
+  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return DISORDER_OK;
+}
+
 int disorder_sample_energies(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf, int32_t n_coils,
                              const void* x, const float* T, const float* Mbe, double* En) {
   if (!ctx) return DISORDER_BAD_ARG;
@@ -818,12 +830,22 @@ int disorder_sample_energies(disorder_ctx ctx, disorder_plan plan, const void* y
   sp.y_N3 = plan->N[2];
   DIS_TRY(dis_encode_segments(ctx, plan, sp, r, (const float2*)y));
   if (ns == 0) return DISORDER_OK;
-  sample_energy_kernel<<<blocks(ns), 256, 0, ctx->stream>>>(r, ns, plan->N[2], n_coils, Mbe, d_en);
-  dis_count(ctx);
-  DIS_CUDA_TRY(cudaGetLastError());
-  DIS_CUDA_TRY(cudaMemcpyAsync(En, d_en, sizeof(double) * ns, cudaMemcpyDeviceToHost, ctx->stream));
-  DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  return DISORDER_OK;
+  return sample_energies_of(ctx, plan, r, n_coils, Mbe, d_en, En);
+}
+
+int disorder_residual_energies(disorder_ctx ctx, disorder_plan plan, const void* r, int32_t n_coils, const float* Mbe,
+                               double* En) {
+  if (!ctx) return DISORDER_BAD_ARG;
+  if (!plan || plan->ctx != ctx) return dis_set_error(ctx, DISORDER_BAD_ARG, "bad plan");
+  if (!r || !En || n_coils < 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "residual energies: bad arguments");
+  DIS_CUDA_TRY(cudaSetDevice(ctx->device));
+  const long long ns = plan->n_samples;
+  if (ns == 0) return DISORDER_OK;
+  Workspace w;
+  DIS_TRY(dis_small(ctx, &w));
+  double* d_en = w.take<double>(ns);
+  if (!d_en) return dis_set_error(ctx, DISORDER_OOM, "residual energies: %lld samples exceed the scratch", ns);
+  return sample_energies_of(ctx, plan, (const float2*)r, n_coils, Mbe, d_en, En);
 }
 
 int disorder_backproject_states(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,

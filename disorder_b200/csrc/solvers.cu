@@ -330,7 +330,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   // plane path does not produce E p: it encodes x at each evaluation.
   std::vector<int> all_segs;
   for (int q = 0; q < plan->n_seg; ++q) all_segs.push_back(q);
-  const bool track = tolType == 6 && !dis_plane_usable(plan, s.C, all_segs);
+  const bool track = (tolType == 6 || s.r_out) && !dis_plane_usable(plan, s.C, all_segs);
   // From an initial guess x0, with r = E x0 - y and without EH.Mb (which
   // decode applies and encodedecode does not), b - EHE(x0) =
   // -constrain(decode(W r) + Ti x0): one encode and one decode replace the
@@ -338,7 +338,8 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   // needed only by the RelativeResidual2Error test with a positive tolerance.
   const bool need_b = tolType == 1 && tol > 0;
   const bool fused_init = x_init && !s.Mb && (track || !need_b);
-  const size_t need = sizeof(float2) * (5 * V + (tolType == 6 || fused_init ? ny : 0) + (track ? ny : 0)) +
+  const bool have_rbuf = tolType == 6 || fused_init || s.r_out;
+  const size_t need = sizeof(float2) * (5 * V + (have_rbuf ? ny : 0) + (track ? ny : 0)) +
                       sizeof(float) * (wm + plan->N[2]) + (1 << 20);
   Workspace ws;
   DIS_TRY(dis_workspace2(ctx, need, &ws));
@@ -349,9 +350,9 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   float2* ehe = ws.take<float2>(V);
   float* wmap = ws.take<float>(wm);
   float* roww = ws.take<float>(plan->N[2]);
-  float2* rbuf = tolType == 6 || fused_init ? ws.take<float2>(ny) : nullptr;
+  float2* rbuf = have_rbuf ? ws.take<float2>(ny) : nullptr;
   float2* ebuf = track ? ws.take<float2>(ny) : nullptr;
-  if (!b || !r || !z || !p || !ehe || !wmap || !roww || ((tolType == 6 || fused_init) && !rbuf) || (track && !ebuf))
+  if (!b || !r || !z || !p || !ehe || !wmap || !roww || (have_rbuf && !rbuf) || (track && !ebuf))
     return dis_set_error(ctx, DISORDER_OOM, "CG workspace");
   DIS_TRY(dis_build_weight_map(ctx, plan, s.We, wmap, 1.f));
   const bool haveRow = s.Mb || s.Mbe;
@@ -393,6 +394,13 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
     sp.y_n3off = 0;
     sp.y_N3 = plan->N[2];
     return dis_encode_segments(ctx, plan, sp, rbuf, s.y);
+  };
+  // the final sample residual for the caller: the tracked one, else a fresh encode
+  auto write_residual = [&](bool tracked) -> int {
+    if (!s.r_out) return DISORDER_OK;
+    if (!tracked) DIS_TRY(encode_residual());
+    DIS_CUDA_TRY(cudaMemcpyAsync(s.r_out, rbuf, sizeof(float2) * ny, cudaMemcpyDeviceToDevice, ctx->stream));
+    return DISORDER_OK;
   };
   // b = constrain(decode(y))   (:46)
   DecodeSpec ds;
@@ -453,7 +461,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   DIS_TRY(red_finish(R, &rs_re, &rs_im));
   *n_en = 0;
   *nn = 0;
-  if (std::hypot(rs_re, rs_im) < 1e-6) return DISORDER_OK;  // :70-75
+  if (std::hypot(rs_re, rs_im) < 1e-6) return write_residual(fused_init);  // :70-75
   if (track) {
     // r = E x0 - y (x0 = 0: r = -y)
     if (x_init) {
@@ -527,6 +535,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
       En[2 * k + 1] = Ecol[2 * k + 1];
     }
   *n_en = ncol;
+  DIS_TRY(write_residual(track));
   DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return DISORDER_OK;
 }

@@ -13,6 +13,7 @@ struct CGSpec {
   const float* P_Se = nullptr;
   const float* C_Ma = nullptr;
   const float* R_Ti = nullptr;
+  float2* r_out = nullptr;  // device, optional: the final sample residual E x - y (encode's layout)
 };
 
 struct LMSpec {

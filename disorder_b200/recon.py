@@ -259,6 +259,7 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
         A = api.Struct(Se=Se)
         est = bool(estT[l])
         use_net = proposal is not None and est and tuple(NXres) == tuple(proposal.D)
+        rres = None  # the sample residual of the image updates at the outlier levels
         nReset, cont = 0, 0
         for n in range(nExtern):
             if nReset == 0 or cont % nReset == 0 or np.all(E.cT):  # solveXT.m:379-384
@@ -271,13 +272,18 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
             else:
                 nX, tolType, tol = 300, "Energy", tolerSolve
             Ex = binned(E, resIso[-1], traLimX) if traLimX is not None else E  # solveXT.m:392
-            xRes, EnX, nn = api.CGsolver(yRes, Ex, EH, A, None, None, xRes, nX, tolType, tol, ctx=ctx)
+            detect = outliers and leff >= 0 and l < n_run - 1
+            if detect and rres is None:
+                rres = ctx.empty((int(nEc[-1]), NXres[2], Ck))
+            xRes, EnX, nn = api.CGsolver(yRes, Ex, EH, A, None, None, xRes, nX, tolType, tol, ctx=ctx,
+                                         residual=rres if detect else None)
             log.add(step="cg", level=l, it=n, iters=nn, tolType=tolType, states=int(Ex.NMs))
-            if outliers and leff >= 0 and l < n_run - 1:
+            if detect:
                 # residual energy per sample and outlier detection after every
-                # image update, the level's last one included (solveXT.m:440-466);
-                # the final level's weights are not used again
-                Re = api.sampleEnergies(yRes, xRes, Ex, EH, ctx=ctx)
+                # image update, the level's last one included (solveXT.m:440-466),
+                # from the residual the image update leaves; the final level's
+                # weights are not used again
+                Re = api.residualSampleEnergies(rres, Ex, EH, ctx=ctx)
                 We_shot = outlier_weights(Re, mSt, n_states, leff)
                 log.add(step="outliers", level=l, it=n, rejected=int(np.sum(We_shot < 1)))
                 # soft shot weights for the next image updates of this level (:478-482)

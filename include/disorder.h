@@ -190,6 +190,18 @@ int disorder_cg_solve(disorder_ctx ctx, disorder_plan plan, const void* y, const
                       void* x_inout, int32_t x_init, int32_t nIt, int32_t tolType, double tol,
                       double* En, int32_t* n_en, int32_t* nn);
 
+/* disorder_cg_solve that also returns the final sample residual
+ * r_out = encode(x) - y (device, samples x N3 x C, encode's layout). CG keeps
+ * that residual beside its vectors, so the caller gets it without another
+ * encode; solveXT.m:443 needs it after every image update at the outlier
+ * levels. No separate reference function. */
+int disorder_cg_solve_residual(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
+                               int32_t n_coils, const float* T, const float* We, const float* Mb,
+                               const float* Mbe, const float* P_Se, const float* C_Ma,
+                               const float* R_Ti, void* x_inout, int32_t x_init, int32_t nIt,
+                               int32_t tolType, double tol, double* En, int32_t* n_en, int32_t* nn,
+                               void* r_out);
+
 /* E=LMsolver(y,E,x,C) (Reconstruction/LMsolver.m:1-226), E.Fs branch, one
  * Levenberg-Marquardt iteration over the motion states.
  * y: device samples (all segments, full readout). Sf: device.
@@ -251,6 +263,11 @@ int disorder_state_energies(disorder_ctx ctx, disorder_plan plan, const void* y,
 int disorder_sample_energies(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
                              int32_t n_coils, const void* x, const float* T, const float* Mbe,
                              double* En);
+/* The same per-sample energies of a residual r that the caller already holds
+ * (device, samples x N3 x C; for example from disorder_cg_solve_residual).
+ * At most 2M samples. */
+int disorder_residual_energies(disorder_ctx ctx, disorder_plan plan, const void* r, int32_t n_coils,
+                               const float* Mbe, double* En);
 int disorder_backproject_states(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
                                 int32_t n_coils, const void* x, const float* T, int32_t n3_lo,
                                 int32_t n3_hi, void* out);

@@ -283,6 +283,29 @@ def test_cg(ctx, tolType, nIt, N, we, tol):
         assert rel(En, Eno) < TOL_SOLVER
 
 
+# CG can return its final sample residual (tracked, or encoded once at the
+# end); it is compared relative to |y| because it shrinks as CG converges
+@pytest.mark.parametrize("tolType,nIt,x_init", [("RelativeResidual2Error", 2, True), ("Energy", 5, True),
+                                                ("RelativeResidual2Error", 3, False)])
+def test_cg_residual_output(ctx, tolType, nIt, x_init):
+    import disorder_b200 as db
+    from oracle import encoding as oenc
+    N = (44, 44, 22)
+    Ed, Eo, sc = _E_pair(ctx, N, 4, 4, seed=31)
+    y = oenc.encode(sc.x_gt.astype(np.complex128), Eo)
+    Se = (1.0 / (np.sum(np.abs(sc.S) ** 2, axis=3) + 1e-9)).astype(np.float32)
+    mbe = (np.arange(N[2]) >= 3).astype(np.float32)
+    r = ctx.empty(y.shape)
+    x, _, _ = db.CGsolver(y.astype(np.complex64), Ed, db.Struct(Mbe=mbe), db.Struct(Se=Se), None, None,
+                          0.5 * sc.x_gt if x_init else None, nIt, tolType, 0.0, ctx=ctx, residual=r)
+    ref = oenc.encode(np.asarray(x).astype(np.complex128), Eo) - y
+    rg = r.numpy()
+    assert np.linalg.norm(rg - ref) < TOL * np.linalg.norm(y)
+    Re = db.api.residualSampleEnergies(r, Ed, db.Struct(Mbe=mbe), ctx=ctx)
+    Re2 = db.api.sampleEnergies(y.astype(np.complex64), x, Ed, db.Struct(Mbe=mbe), ctx=ctx)
+    assert rel(Re, Re2) < 1e-3
+
+
 def test_lm_step(ctx):
     import disorder_b200 as db
     from oracle import encoding as oenc
