@@ -55,6 +55,8 @@ SIGNATURES = [
     ("disorder_upload", C.c_int, [VP, VP, C.c_size_t, C.POINTER(VP)]),
     ("disorder_download", C.c_int, [VP, VP, VP, C.c_size_t]),
     ("disorder_kernel_launches", C.c_int64, [VP]),
+    ("disorder_workspace_bytes", C.c_int64, [VP]),
+    ("disorder_ctx_inject_fault", C.c_int, [VP, I32]),
     ("disorder_event_record", C.c_int, [VP, I32]),
     ("disorder_event_elapsed", C.c_int, [VP, I32, I32, FP]),
     ("disorder_plan_create", C.c_int, [VP, C.POINTER(GridDesc), C.POINTER(SamplingDesc), C.POINTER(VP)]),

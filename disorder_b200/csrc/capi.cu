@@ -24,6 +24,10 @@ int dis_set_error(disorder_ctx_s* ctx, int status, const char* fmt, ...) {
 
 static int grow(disorder_ctx_s* ctx, void** buf, size_t* cap, size_t bytes) {
   if (bytes <= *cap && *buf) return DISORDER_OK;
+  if (ctx->fault == DISORDER_FAULT_OOM) {
+    ctx->fault = DISORDER_FAULT_NONE;
+    return dis_set_error(ctx, DISORDER_OOM, "cudaMalloc of %zu bytes failed: injected fault", bytes);
+  }
   if (*buf) {
     DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     cudaFree(*buf);
@@ -122,6 +126,10 @@ int disorder_ctx_create(int device, disorder_ctx* out) {
     }
   }
   cudaGetLastError();
+  // the static scratch of disorder_sinc_rigid_transform_static: resolving its
+  // address here loads its module and commits it on this device, so that
+  // entry point makes no allocation (a failure only disables that entry point)
+  dis_static_scratch_resolve(&ctx->static_scratch, &ctx->static_scratch_bytes);
   if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess || cudaMemset(ctx->d_err, 0, 256) != cudaSuccess) {
     cudaGetLastError();
     if (ctx->d_err) cudaFree(ctx->d_err);
@@ -262,6 +270,18 @@ int disorder_memset(disorder_ctx ctx, void* dst, int value, size_t bytes) {
 }
 
 int64_t disorder_kernel_launches(disorder_ctx ctx) { return ctx ? ctx->launches : -1; }
+
+int disorder_ctx_inject_fault(disorder_ctx ctx, int32_t fault) {
+  CTX_CHECK(ctx);
+  if (fault < DISORDER_FAULT_NONE || fault > DISORDER_FAULT_OOM)
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "inject_fault: unknown fault %d", fault);
+  ctx->fault = fault;
+  return DISORDER_OK;
+}
+
+int64_t disorder_workspace_bytes(disorder_ctx ctx) {
+  return ctx ? (int64_t)(ctx->ws_bytes + ctx->ws2_bytes + ctx->small_bytes) : -1;
+}
 
 int disorder_event_record(disorder_ctx ctx, int32_t slot) {
   CTX_CHECK(ctx);

@@ -1,7 +1,7 @@
 // Coil stage of the encoding operators: coil expansion, the unitary 2-D DFT
 // over the phase encodes, per-segment sample gather/scatter, k-space
 // weighting, and the conj-coil combination (Reconstruction/encode.m:90-136,
-// decode.m:175-233, encodedecode.m:91-178). The per-sample DFT rows of the
+// decode.m:42-58,78-85, encodedecode.m:91-178). The per-sample DFT rows of the
 // reference (Fs{1}, Fs{2}: rows of build1DFTM(N,1)) are evaluated as a full
 // FFT along dim 1 followed by an FFT along dim 2 and a gather of each
 // segment's samples, which is the same linear map.

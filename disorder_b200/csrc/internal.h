@@ -26,6 +26,11 @@ struct disorder_ctx_s {
   size_t small_bytes = 0;
   cudaEvent_t ev[16] = {};
   int* d_err = nullptr;  // device error word of bounded in-kernel waits (0: none)
+  // the static scratch array of disorder_sinc_rigid_transform_static on this
+  // device, resolved at context creation (null if that failed)
+  void* static_scratch = nullptr;
+  size_t static_scratch_bytes = 0;
+  int fault = 0;  // one-shot injected fault (disorder_ctx_inject_fault)
 };
 
 // Workspace bump allocator on top of the context's cached buffer.
@@ -166,6 +171,11 @@ int dis_build_tables_into(disorder_ctx_s* ctx, const disorder_plan_s* plan, cons
                           char* base, size_t cap, Tables* tb);
 // per-slot scalars into a caller array (no heap)
 void dis_slot_params_into(const float* T, int n_states, int di, SlotParams* out);
+// bytes dis_build_tables_into places in its region for ns slots
+size_t dis_static_table_bytes(const disorder_plan_s* plan, int ns);
+// device address of the static scratch of disorder_sinc_rigid_transform_static
+// on the current device (noalloc.cu); called once when a context is created
+int dis_static_scratch_resolve(void** addr, size_t* bytes);
 
 // transform drivers (ops.cu)
 int dis_forward_transform(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* x, long long x_s,

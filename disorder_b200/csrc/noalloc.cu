@@ -8,8 +8,14 @@
 // from its own allocator, where a cudaMalloc can fail once that budget is
 // taken and, besides, synchronises the device. For them this entry point keeps
 // all of its scratch (the phase tables and the per-state scalars) in one
-// file-scope device array of fixed size, kStaticScratchBytes (32 MiB), that
-// every GPU which loads this library holds until the process exits.
+// file-scope device array of fixed size, kStaticScratchBytes (32 MiB).
+//
+// The array's device address is resolved once per context, when the context
+// is created (dis_static_scratch_resolve, called by disorder_ctx_create with
+// the context's device current). That first cudaGetSymbolAddress also loads
+// the module holding the array, which commits its 32 MiB on that device; the
+// device keeps them until the process exits. The entry point itself then
+// makes no allocation and loads no data module.
 #include <cstring>
 
 #include "internal.h"
@@ -19,21 +25,24 @@ namespace {
 constexpr size_t kStaticScratchBytes = 32ull << 20;
 __device__ __align__(256) unsigned char g_scratch[kStaticScratchBytes];
 
-constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// bytes the tables of n states need in the static scratch (with the 256-byte
-// rounding of every sub-allocation)
-size_t table_bytes(const disorder_plan_s* p, int n) {
-  auto r = [](size_t b) { return (b + 255) & ~size_t(255); };
-  const size_t N0 = p->N[0], N1 = p->N[1], N2 = p->N[2];
-  size_t b = r(15 * sizeof(double) * n);
-  b += 2 * (r(sizeof(float2) * N0 * N1 * n) + r(sizeof(float2) * N2 * N0 * n) + r(sizeof(float2) * N1 * N2 * n));
-  b += r(sizeof(float2) * N0 * n) + r(sizeof(float2) * N1 * n) + r(sizeof(float2) * N2 * n);
-  return b;
-}
-
 }  // namespace
+
+// In host code g_scratch names a host-side stand-in, not device memory: a
+// kernel handed it would fault or read the wrong memory. The runtime gives the
+// array's address on the current device.
+int dis_static_scratch_resolve(void** addr, size_t* bytes) {
+  *addr = nullptr;
+  *bytes = 0;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    return DISORDER_CUDA_ERR;
+  }
+  *addr = p;
+  *bytes = kStaticScratchBytes;
+  return DISORDER_OK;
+}
 
 extern "C" int disorder_sinc_rigid_transform_static(disorder_ctx ctx, disorder_plan plan, const void* x,
                                                     int32_t x_states, const float* T, int32_t n_states, int32_t di,
@@ -50,13 +59,19 @@ extern "C" int disorder_sinc_rigid_transform_static(disorder_ctx ctx, disorder_p
   if (n_states > kMaxStaticSlots)
     return dis_set_error(ctx, DISORDER_BAD_ARG, "sinc_rigid_transform_static: at most %d states per call",
                          kMaxStaticSlots);
-  const size_t need = table_bytes(plan, n_states);
+  const size_t need = dis_static_table_bytes(plan, n_states);
   if (need > kStaticScratchBytes)
     return dis_set_error(ctx, DISORDER_BAD_ARG,
                          "sinc_rigid_transform_static: %d states of a %dx%dx%d grid need %zu bytes of scratch; "
                          "the static scratch holds %zu bytes (use fewer states per call)",
                          n_states, plan->N[0], plan->N[1], plan->N[2], need, kStaticScratchBytes);
-  SlotParams sp[kMaxStaticSlots];
+  if (!ctx->static_scratch)
+    return dis_set_error(ctx, DISORDER_CUDA_ERR,
+                         "sinc_rigid_transform_static: the static scratch address could not be resolved when the "
+                         "context was created");
+  // per-state scalars staged in thread-local static storage: no heap, and no
+  // large stack frame on the caller's thread
+  static thread_local SlotParams sp[kMaxStaticSlots];
   dis_slot_params_into(T, n_states, di, sp);
   for (int s = 0; s < n_states; ++s)
     if (sp[s].flip[0] || sp[s].flip[1] || sp[s].flip[2])
@@ -65,20 +80,9 @@ extern "C" int disorder_sinc_rigid_transform_static(disorder_ctx ctx, disorder_p
                            "(state %d); use disorder_sinc_rigid_transform",
                            s);
   DIS_CUDA_TRY(cudaSetDevice(ctx->device));
-  if (ctx->device < 0 || ctx->device >= kMaxDevices)
-    return dis_set_error(ctx, DISORDER_BAD_ARG, "sinc_rigid_transform_static: device %d", ctx->device);
-  // set-up, once per device and with that device current: the host-side name
-  // g_scratch is not a device address, so take the address from the runtime
-  if (!g_scratch_addr[ctx->device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess || !p)
-      return dis_set_error(ctx, DISORDER_CUDA_ERR, "cudaGetSymbolAddress(static scratch): %s", cudaGetErrorString(e));
-    g_scratch_addr[ctx->device] = p;
-  }
   Tables tb;
-  const int st = dis_build_tables_into(ctx, plan, sp, n_states, (char*)g_scratch_addr[ctx->device],
-                                       kStaticScratchBytes, &tb);
+  const int st = dis_build_tables_into(ctx, plan, sp, n_states, (char*)ctx->static_scratch,
+                                       ctx->static_scratch_bytes, &tb);
   if (st == DISORDER_OOM)
     return dis_set_error(ctx, DISORDER_BAD_ARG, "sinc_rigid_transform_static: tables exceed the static scratch");
   if (st != DISORDER_OK) return st;

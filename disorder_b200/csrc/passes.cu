@@ -296,8 +296,8 @@ struct FlipArgs {
   FFTPlan plan;
 };
 
-// out = shift(in, h): integer h -> circular index shift (shifting.m:200-204),
-// otherwise the DFT phase ramp exp(-i k h) (shifting.m:210-216).
+// out = shift(in, h): integer h -> circular index shift (shifting.m:29-37),
+// otherwise the DFT phase ramp exp(-i k h) (shifting.m:38-47).
 DIS_D float2* shift_tile(float2* src, float2* dst, float2* scr, float h, const FlipArgs& a,
                          const float2* tw, int tid, int nthr) {
   const int n = a.plan.n, L = a.L, P = a.pitch;

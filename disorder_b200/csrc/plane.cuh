@@ -6,7 +6,7 @@
 // of a full 2-D FFT and a gather we FFT the plane's columns along n1 (all ky
 // are used) and evaluate the kz sum only at the segment's samples:
 //   y_i = sum_{n2} W_N2^{kz_i n2} X[ky_i, n2],  X = FFT_1(S_c z).
-// The adjoint (decode.m:189-232) rebuilds each column from the samples,
+// The adjoint (decode.m:42-58,78-85) rebuilds each column from the samples,
 //   X[ky, n2] = sum_{i in row ky} w_i y_i conj(W_N2^{kz_i n2}),
 // inverse-FFTs it along n1, multiplies by conj(S_c) and sums over coils in
 // registers. The sample values of all coils live in shared memory, so the

@@ -3,7 +3,7 @@
 //    mirroring): per changed axis DFT/Nin, centred crop or zero-pad, inverse
 //    DFT*Nout;
 //  - sample gather for a pyramid level (the k-space crop of downsampleOperators,
-//    Methods/downsampleOperators.m:53,67, applied to a sample list);
+//    Methods/downsampleOperators.m:48-51, applied to a sample list);
 //  - coil compression (Methods/compressCoils.m:76-118): Gram matrix on the
 //    device (double accumulation), Hermitian eigendecomposition on the host
 //    (cyclic Jacobi), compression products on the device;

@@ -461,6 +461,8 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   DIS_TRY(red_finish(R, &rs_re, &rs_im));
   *n_en = 0;
   *nn = 0;
+  if (!std::isfinite(rs_re) || !std::isfinite(rs_im))
+    return dis_set_error(ctx, DISORDER_NONFINITE, "CG: non-finite initial residual (non-finite y, x0 or weights)");
   if (std::hypot(rs_re, rs_im) < 1e-6) return write_residual(fused_init);  // :70-75
   if (track) {
     // r = E x0 - y (x0 = 0: r = -y)
@@ -480,6 +482,8 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
     dis_count(ctx);
     double pa_re = 0, pa_im = 0;
     DIS_TRY(red_finish(R, &pa_re, &pa_im));
+    if (!std::isfinite(pa_re) || !std::isfinite(pa_im))
+      return dis_set_error(ctx, DISORDER_NONFINITE, "CG: non-finite <p, EHE p> at iteration %d", n);
     // g = rsold / <p, EHE>  (:82)
     const double den = pa_re * pa_re + pa_im * pa_im;
     const double g_re = (rs_re * pa_re + rs_im * pa_im) / den;
@@ -491,6 +495,8 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
     dis_count(ctx);
     double rn_re = 0, rn_im = 0;
     DIS_TRY(red_finish(R, &rn_re, &rn_im));
+    if (!std::isfinite(rn_re) || !std::isfinite(rn_im))
+      return dis_set_error(ctx, DISORDER_NONFINITE, "CG: non-finite residual at iteration %d", n);
     if (track) {
       caxpy_kernel<<<blocks, 256, 0, ctx->stream>>>(rbuf, ebuf, make_float2((float)g_re, (float)g_im), ny);
       dis_count(ctx);
@@ -690,6 +696,9 @@ int dis_lm_step(disorder_ctx_s* ctx, const disorder_plan_s* plan, const LMSpec& 
     sums.assign((size_t)n * 28, 0.0);
     DIS_CUDA_TRY(cudaMemcpyAsync(sums.data(), d_out, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (double v : sums)
+      if (!std::isfinite(v))
+        return dis_set_error(ctx, DISORDER_NONFINITE, "LM: non-finite residual or Jacobian sums (non-finite y or x?)");
     for (int j = 0; j < n; ++j) {
       const int q = st[j];
       EnPrev[q] = sums[j * 28] / NElY;  // :82-83,93

@@ -1,5 +1,5 @@
 // Phase factors of the sinc rigid transform
-// (Methods/precomputeFactorsSincRigidTransform.m:158-240, gr=1, sh=1).
+// (Methods/precomputeFactorsSincRigidTransform.m:42-125, gr=1, sh=1).
 // Per-state scalars (wrapped angles, tan/sin/cos) are formed on the host in
 // double precision; the per-element factors exp(i*phase) are evaluated on the
 // device in double precision and rounded to single. The 1/N of the inverse
@@ -146,52 +146,76 @@ int build_seeds(disorder_ctx_s* ctx, const disorder_plan_s* plan, const double* 
 
 }  // namespace
 
-void dis_slot_params_into(const float* T, int n_states, int di, SlotParams* out) {
-  const double sd = (di == 1) ? -1.0 : 1.0;
-  const double sdm = (di == 1) ? 1.0 : -1.0;
-  for (int s = 0; s < n_states; ++s) {
-    SlotParams& p = out[s];
-    for (int a = 0; a < 3; ++a) p.t[a] = sd * (double)T[a * n_states + s];
-    for (int m = 0; m < 3; ++m) {
-      double th = wrap_to_pi((double)T[(3 + m) * n_states + s]);
-      p.flip[m] = std::fabs(th) > M_PI / 2 ? 1 : 0;
-      th = wrap_to_pi_half(th);
-      const double t2 = std::tan(th / 2);
-      p.tau[m] = sdm * t2;
-      p.sig[m] = sd * std::sin(th);
-      p.g2[m] = (1 + t2 * t2) / 2;
-      p.g3[m] = std::cos(th);
-    }
+// Per-state scalars of one transform (precomputeFactorsSincRigidTransform.m:45-65)
+// from T(s, :) of an n_states x 6 parameter-major array.
+static void slot_params_one(const float* T, int n_states, int s, int di, SlotParams* p) {
+  const double sd = (di == 1) ? -1.0 : 1.0;    // (-1)^di
+  const double sdm = (di == 1) ? 1.0 : -1.0;   // (-1)^(di-1)
+  for (int a = 0; a < 3; ++a) p->t[a] = sd * (double)T[a * n_states + s];
+  for (int m = 0; m < 3; ++m) {
+    double th = wrap_to_pi((double)T[(3 + m) * n_states + s]);
+    p->flip[m] = std::fabs(th) > M_PI / 2 ? 1 : 0;
+    th = wrap_to_pi_half(th);
+    const double t2 = std::tan(th / 2);
+    p->tau[m] = sdm * t2;
+    p->sig[m] = sd * std::sin(th);
+    p->g2[m] = (1 + t2 * t2) / 2;
+    p->g3[m] = std::cos(th);
   }
+}
+
+void dis_slot_params_into(const float* T, int n_states, int di, SlotParams* out) {
+  for (int s = 0; s < n_states; ++s) slot_params_one(T, n_states, s, di, &out[s]);
 }
 
 void dis_slot_params(const float* T, int n_states, const int* slots, int n_slots, int di,
                      std::vector<SlotParams>* out) {
   out->resize(n_slots);
-  const double sd = (di == 1) ? -1.0 : 1.0;    // (-1)^di
-  const double sdm = (di == 1) ? 1.0 : -1.0;   // (-1)^(di-1)
-  for (int j = 0; j < n_slots; ++j) {
-    const int s = slots ? slots[j] : j;
-    SlotParams& p = (*out)[j];
-    for (int a = 0; a < 3; ++a) p.t[a] = sd * (double)T[a * n_states + s];
-    for (int m = 0; m < 3; ++m) {
-      double th = wrap_to_pi((double)T[(3 + m) * n_states + s]);
-      p.flip[m] = std::fabs(th) > M_PI / 2 ? 1 : 0;
-      th = wrap_to_pi_half(th);
-      const double t2 = std::tan(th / 2);
-      p.tau[m] = sdm * t2;
-      p.sig[m] = sd * std::sin(th);
-      p.g2[m] = (1 + t2 * t2) / 2;
-      p.g3[m] = std::cos(th);
-    }
+  for (int j = 0; j < n_slots; ++j) slot_params_one(T, n_states, slots ? slots[j] : j, di, &(*out)[j]);
+}
+
+// Places the forward/inverse tables of ns slots (no derivative factors, no
+// seeds) in ws: the per-slot scalars d, then e2/e3 per rotation, then e1 per
+// axis. The one layout both dis_static_table_bytes and dis_build_tables_into
+// use. Returns false when ws runs out.
+static bool static_table_layout(const disorder_plan_s* plan, int ns, Workspace* ws, Tables* tb, double** d) {
+  const int* N = plan->N;
+  *d = ws->take<double>(15 * (size_t)ns);
+  if (!*d) return false;
+  for (int m = 0; m < 3; ++m) {
+    const int a1 = TR0[m], a2 = TR1[m];
+    tb->e2s[m] = (long long)N[a1] * N[a2];
+    tb->e3s[m] = (long long)N[a2] * N[a1];
+    tb->e2[m] = ws->take<float2>(tb->e2s[m] * ns);
+    tb->e3[m] = ws->take<float2>(tb->e3s[m] * ns);
+    tb->g2[m] = tb->g3[m] = nullptr;
+    if (!tb->e2[m] || !tb->e3[m]) return false;
   }
+  for (int a = 0; a < 3; ++a) {
+    tb->e1s[a] = N[a];
+    tb->e1[a] = ws->take<float2>((size_t)N[a] * ns);
+    if (!tb->e1[a]) return false;
+  }
+  return true;
+}
+
+size_t dis_static_table_bytes(const disorder_plan_s* plan, int ns) {
+  // a counting workspace: a non-null base that is never dereferenced
+  Workspace ws;
+  ws.base = reinterpret_cast<char*>(256);
+  ws.cap = ~size_t(0) >> 1;
+  ws.off = 0;
+  Tables tb;
+  double* d = nullptr;
+  static_table_layout(plan, ns, &ws, &tb, &d);
+  return ws.off;
 }
 
 // Forward/inverse transform tables for ns <= kMaxStaticSlots slots placed in
 // the caller's region [base, base+cap) with no heap use on the host or the
-// device: the per-slot scalars are staged in a stack array. Returns OOM when
-// the tables do not fit in cap bytes. Flip-slot lists are not built (the
-// caller rejects rotations beyond 90 degrees).
+// device: the per-slot scalars are staged in a thread-local static array.
+// Returns OOM when the tables do not fit in cap bytes. Flip-slot lists are not
+// built (the caller rejects rotations beyond 90 degrees).
 int dis_build_tables_into(disorder_ctx_s* ctx, const disorder_plan_s* plan, const SlotParams* sp, int ns,
                           char* base, size_t cap, Tables* tb) {
   if (ns < 1 || ns > kMaxStaticSlots) return dis_set_error(ctx, DISORDER_BAD_ARG, "tables: %d slots", ns);
@@ -200,7 +224,9 @@ int dis_build_tables_into(disorder_ctx_s* ctx, const disorder_plan_s* plan, cons
   ws.cap = cap;
   ws.off = 0;
   const int* N = plan->N;
-  double h[15 * kMaxStaticSlots];
+  double* d = nullptr;
+  if (!static_table_layout(plan, ns, &ws, tb, &d)) return DISORDER_OOM;
+  static thread_local double h[15 * kMaxStaticSlots];
   for (int j = 0; j < ns; ++j)
     for (int m = 0; m < 3; ++m) {
       h[(0 * 3 + m) * ns + j] = sp[j].tau[m];
@@ -209,20 +235,12 @@ int dis_build_tables_into(disorder_ctx_s* ctx, const disorder_plan_s* plan, cons
       h[(3 * 3 + m) * ns + j] = sp[j].g3[m];
       h[(4 * 3 + m) * ns + j] = sp[j].t[m];
     }
-  double* d = ws.take<double>(15 * (size_t)ns);
-  if (!d) return DISORDER_OOM;
   // a pageable-source copy is staged before the call returns
   DIS_CUDA_TRY(cudaMemcpyAsync(d, h, 15 * (size_t)ns * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   tb->n_slots = ns;
   const int blocks = 2 * ctx->sm_count;
   for (int m = 0; m < 3; ++m) {
     const int a1 = TR0[m], a2 = TR1[m];
-    tb->e2s[m] = (long long)N[a1] * N[a2];
-    tb->e3s[m] = (long long)N[a2] * N[a1];
-    tb->e2[m] = ws.take<float2>(tb->e2s[m] * ns);
-    tb->e3[m] = ws.take<float2>(tb->e3s[m] * ns);
-    tb->g2[m] = tb->g3[m] = nullptr;
-    if (!tb->e2[m] || !tb->e3[m]) return DISORDER_OOM;
     shear_table_kernel<<<blocks, 256, 0, ctx->stream>>>(tb->e2[m], nullptr, N[a1], N[a2], plan->d_kG[a1],
                                                         plan->d_rG[a2], d + (0 * 3 + m) * ns, d + (2 * 3 + m) * ns,
                                                         +1, 1.0 / N[a1], ns);
@@ -232,9 +250,6 @@ int dis_build_tables_into(disorder_ctx_s* ctx, const disorder_plan_s* plan, cons
     dis_count(ctx, 2);
   }
   for (int a = 0; a < 3; ++a) {
-    tb->e1s[a] = N[a];
-    tb->e1[a] = ws.take<float2>((size_t)N[a] * ns);
-    if (!tb->e1[a]) return DISORDER_OOM;
     trans_table_kernel<<<blocks, 256, 0, ctx->stream>>>(tb->e1[a], N[a], plan->d_kG[a], d + (4 * 3 + a) * ns, ns);
     dis_count(ctx);
   }

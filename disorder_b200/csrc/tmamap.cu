@@ -82,6 +82,16 @@ bool dis_tmap_volumes(CUtensorMap* m, const void* base, const int* N, int axis, 
   return r == CUDA_SUCCESS;
 }
 
+// an injected wait fault (disorder_ctx_inject_fault) applies to the next
+// TMA pass only
+static void take_fault(disorder_ctx_s* ctx, fp::TArgs& t) {
+  if (ctx->fault == DISORDER_FAULT_TMA_WAIT) {
+    ctx->fault = DISORDER_FAULT_NONE;
+    t.skip_loads = 1;
+    t.wait_limit = 1u << 12;
+  }
+}
+
 bool dis_fast_tma_line(disorder_ctx_s* ctx, const LinePassArgs& a) {
   if (!tma_enabled() || !ctx->d_err) return false;
   if (a.axis == 0 || a.accumulate || a.in1 || a.out1 || a.c01 != P_ZERO) return false;
@@ -104,6 +114,7 @@ bool dis_fast_tma_line(disorder_ctx_s* ctx, const LinePassArgs& a) {
   t.wmap = nullptr;
   t.a = a;
   t.err = ctx->d_err;
+  take_fault(ctx, t);
   return launch_size(n, 0, in, out, t, a.tw, shared_input, ctx->stream);
 }
 
@@ -136,6 +147,7 @@ bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, cons
     t.kyv = plan->d_ky;
     t.kzv = plan->d_kz;
   }
+  take_fault(ctx, t);
   return launch_size(a.N2, 1, m, m, t, tw, 0, ctx->stream);
 }
 
@@ -160,6 +172,7 @@ bool coil_tma(disorder_ctx_s* ctx, int kind, const CoilArgs& a, float2* A, const
   t.perm = plan->d_perm;
   t.kyv = plan->d_ky;
   t.kzv = plan->d_kz;
+  take_fault(ctx, t);
   return launch_size(a.N2, kind, m, m, t, plan->d_tw[1], 0, ctx->stream);
 }
 }  // namespace

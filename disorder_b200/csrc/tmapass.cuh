@@ -103,6 +103,12 @@ struct TArgs {
   const float* wmap;  // KIND 1: [seg][N0][N_pass]
   LinePassArgs a;     // KIND 0: seeds
   int* err;           // device error word (set to 1 when a wait runs out)
+  // bound of every tile wait, in try_wait rounds (each suspends for a short
+  // hardware-defined time; the default is of the order of a second)
+  unsigned wait_limit = 1u << 20;
+  // failure-path testing (disorder_ctx_inject_fault): issue no tile load, so
+  // the first wait of every CTA runs out with nothing in flight
+  int skip_loads = 0;
   // KIND 2 / 3: per-segment CSR of the samples by ky row, sample rows and
   // the sample array y[ld*(n3 + n3off) + ld*N3y*c + i]
   const int* rowptr;
@@ -157,6 +163,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     it.nv = min(16, t.Nv[0] - it.ca);
   };
   auto issue = [&](const PItem& it, int c, float2* st, uint64_t* bar) {
+    if (t.skip_loads) return;
     mbar_expect_tx(bar, P::BOX_BYTES);
     const int w = KIND >= 1 ? it.slot * C + c : (shared_input ? 0 : it.slot);
     tma_load_tile(st, &in_map, it.ca, t.axis == 2 ? it.cb : 0, t.axis == 1 ? it.cb : 0, w, bar);
@@ -182,12 +189,12 @@ __global__ void __launch_bounds__(kThreads, 3)
     if (KIND == 1)
       wm = t.wmap + ((long long)t.slot_seg[cur.slot] * t.Nv[0] + cur.ca + (valid ? li : 0)) * t.Nv[t.axis];
     // bounded wait for the tile (each try_wait suspends for a short
-    // hardware-defined time; the bound is of the order of a second)
+    // hardware-defined time; the default bound is of the order of a second)
     bool late = false;
     if (LOAD) {
       uint32_t spins = 0;
       while (!mbar_try_wait(&mbar[j & 1], (uint32_t)((j >> 1) & 1))) {
-        if (++spins > (1u << 20)) {
+        if (++spins > t.wait_limit) {
           late = true;
           break;
         }
@@ -197,6 +204,12 @@ __global__ void __launch_bounds__(kThreads, 3)
     if (__syncthreads_or(late)) {
       if (tid == 0) {
         atomicExch(t.err, 1);
+        // the only load that can be in flight is item j's (item j+1's is
+        // issued after this wait): give it another bounded wait to land
+        // before the CTA's shared memory is released, then drain the stores
+        if (LOAD && !t.skip_loads)
+          for (uint32_t k = 0; k < t.wait_limit && !mbar_try_wait(&mbar[j & 1], (uint32_t)((j >> 1) & 1)); ++k) {
+          }
         bulk_wait0();
       }
       return;

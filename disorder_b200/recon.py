@@ -176,12 +176,31 @@ def outlier_weights(Re, sweeps, n_sweeps, leff, percRobustShot=(0.125, 0.25), en
     return np.minimum(tail / ((1.0 - enerRobustShot) / n_sweeps), 1.0)
 
 
+def unsampled_states(nEc, n_states):
+    """The motion states with no samples in a level's sampling (the check of
+    Reconstruction/solveXT.m:355): any such state means the acquisition is
+    probably not DISORDER, and the reference returns without correcting."""
+    return np.flatnonzero(np.diff(np.asarray(nEc, np.int64))[:n_states] == 0)
+
+
 def _sample_weights(We_shot, mSt, n_states):
     """Per-sample EH.We from shot weights; outer samples keep 1 (solveXT.m:480-481)."""
     w = np.ones(len(mSt), np.float32)
     inner = np.asarray(mSt) < n_states
     w[inner] = np.asarray(We_shot)[np.asarray(mSt)[inner]]
     return w
+
+
+def _uncorrected(ctx, S, y, H, n_states, N, tolerSolve):
+    """CGsolver at zero motion and full resolution to the energy tolerance
+    (solveXT.m:243), preconditioned by A.Se (solveXT.m:231-233)."""
+    ky, kz, nEc, mSt, _ = level_sampling(H, n_states, N[:2])
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    E = api.Struct(Tr=np.zeros((n_states, 6), np.float32), NMs=n_states, NSe=n_states + 1, Sf=S,
+                   grids=api.generateTransformGrids(N, N, cent, sh=1), ky=ky, kz=kz, nEc=nEc, mSt=mSt)
+    A = api.Struct(Se=api.precondition_weights(S, 1e-9, ctx=ctx))
+    x, _, _ = api.CGsolver(y, E, None, A, None, None, None, 300, "Energy", tolerSolve, ctx=ctx)
+    return x
 
 
 class ReconLog:
@@ -192,6 +211,62 @@ class ReconLog:
     def add(self, **kw):
         kw["t"] = time.perf_counter() - self.t0
         self.events.append(kw)
+
+
+def reset_schedule():
+    """The motion-convergence resets of solveXT.m:379-384 as a closure: call
+    it at the start of every outer iteration with the current convergence
+    flags; it returns True when they are to be cleared."""
+    st = {"nReset": 0, "cont": 0}
+
+    def due(cT):
+        reset = st["nReset"] == 0 or st["cont"] % st["nReset"] == 0 or bool(np.all(cT))
+        if reset:
+            st["nReset"] += 1
+            st["cont"] = 0
+        st["cont"] += 1
+        return reset
+
+    return due
+
+
+def alternating_reconstruction(ctx, S, y, ky, kz, nEc, mSt, n_states, N, n_outer=10, n_cg=3, n_lm=1, winit=1e-3,
+                               tL=(0.05, 0.02), reg=1e-9, log=None, on_stage=None):
+    """Aligned reconstruction at one resolution with a fixed schedule (the
+    small simulation case): n_outer times an image update by CGsolver, n_cg
+    iterations from the current image with the preconditioner
+    A.Se = 1 / (sum_c |S_c|^2 + reg) (solveXT.m:231-233,431), then a motion
+    update by n_lm LMsolver iterations (solveXT.m:507), with the
+    motion-convergence resets of solveXT.m:379-384.
+
+    S: coil maps (N1,N2,N3,C) device array; y: samples (Ns,N3,C) ordered by
+    segment as (ky, kz, nEc, mSt) list them; n_states motion states, then the
+    outer segment. on_stage(stage, n, x, E) is called after every update
+    ("cg" or "lm", outer iteration n). Returns (x device volume, T, log)."""
+    log = log if log is not None else ReconLog()
+    N = tuple(int(n) for n in N)
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    grids = api.generateTransformGrids(N, N, cent, sh=1)
+    x = ctx.empty(N)
+    ctx.check(ctx.lib.disorder_memset(ctx.h, x.ptr, 0, x.nbytes))
+    E = api.Struct(Tr=np.zeros((n_states, 6), np.float32), NMs=n_states, NSe=len(nEc) - 1, Sf=S, grids=grids,
+                   ky=ky, kz=kz, nEc=nEc, mSt=mSt, w=np.full(n_states, winit, np.float32),
+                   cT=np.zeros(n_states, bool), winit=winit, tL=list(tL))
+    A = api.Struct(Se=api.precondition_weights(S, reg, ctx=ctx))
+    due = reset_schedule()
+    for n in range(n_outer):
+        if due(E.cT):
+            E.cT = np.zeros(n_states, bool)
+        x, _, nn = api.CGsolver(y, E, None, A, None, None, x, n_cg, "RelativeResidual2Error", 0.0, ctx=ctx)
+        log.add(step="cg", level=0, it=n, iters=nn, states=n_states)
+        if on_stage:
+            on_stage("cg", n, x, E)
+        for _ in range(n_lm):
+            E = api.LMsolver(y, E, x, ctx=ctx)
+        log.add(step="lm", level=0, it=n, unconverged=int(np.sum(~E.cT)), energy=float(np.sum(E.En)))
+        if on_stage:
+            on_stage("lm", n, x, E)
+    return x, E.Tr, log
 
 
 def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), perc=16, resolMax=4.0,
@@ -234,6 +309,14 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
         xRes = api.resampling(x, NXres, ctx=ctx)
         SRes = api.resampling(Sc, NXres, ctx=ctx)
         ky, kz, nEc, mSt, src = level_sampling(H, n_states, NXres[:2])
+        empty = unsampled_states(nEc, n_states)
+        if empty.size:
+            # "Probably not DISORDER, returning without performing
+            # corrections" (solveXT.m:355): the result is the uncorrected
+            # reconstruction of solveXT.m:243 (zero motion, full resolution)
+            log.add(step="abort", level=l, states=[int(v) for v in empty],
+                    reason="Probably not DISORDER: motion states without samples at this level")
+            return _uncorrected(ctx, Sc, yc, H, n_states, N, tolerSolve), np.zeros((n_states, 6), np.float32), log
         scale = math.sqrt(NXres[0] / N[0] * NXres[1] / N[1])
         ysel = api.gather_samples(yc, src, scale, ctx=ctx)
         yRes = api.resampling(ysel, (len(src), NXres[2], Ck), ctx=ctx) if NXres[2] != N[2] else ysel

@@ -70,6 +70,24 @@ int disorder_download(disorder_ctx ctx, const void* dptr, void* host, size_t byt
 int disorder_memset(disorder_ctx ctx, void* dst, int value, size_t bytes);
 /* number of kernels this context has launched since creation */
 int64_t disorder_kernel_launches(disorder_ctx ctx);
+/* Failure-path testing (no reference counterpart): arm one fault on the
+ * context, taken by the next operation that reaches it and then cleared.
+ * DISORDER_FAULT_TMA_WAIT: the next TMA line pass issues no tile loads, so
+ *   its bounded tile waits run out (after a few milliseconds) with nothing in
+ *   flight; the pass stops early and the next disorder_synchronize returns
+ *   DISORDER_TIMEOUT. The context stays usable.
+ * DISORDER_FAULT_OOM: the next workspace growth fails as a failed cudaMalloc
+ *   would, and the call returns DISORDER_OOM. */
+typedef enum {
+  DISORDER_FAULT_NONE = 0,
+  DISORDER_FAULT_TMA_WAIT = 1,
+  DISORDER_FAULT_OOM = 2
+} disorder_fault;
+int disorder_ctx_inject_fault(disorder_ctx ctx, int32_t fault);
+/* bytes of device workspace the context holds (operator, solver and reduction
+ * buffers it grows on demand and keeps until disorder_ctx_destroy); a
+ * diagnostic with no reference counterpart */
+int64_t disorder_workspace_bytes(disorder_ctx ctx);
 /* CUDA-event timing on the context's stream (no reference counterpart):
  * disorder_event_record(ctx, slot) records event `slot` (0..15);
  * disorder_event_elapsed(ctx, a, b, &ms) synchronises on b and returns the
@@ -103,7 +121,7 @@ int disorder_plan_destroy(disorder_plan plan);
 /* ---- sinc rigid transform ----
  * [x,xB]=sincRigidTransform(x,et,di,F,FH,sumR,useFull) with et from
  * precomputeFactorsSincRigidTransform(kG,rkG,T,di,0,1,1)
- * (Methods/sincRigidTransform.m:1-116; Methods/precomputeFactorsSincRigidTransform.m:24-249).
+ * (Methods/sincRigidTransform.m:1-116; Methods/precomputeFactorsSincRigidTransform.m:24-133).
  * x: device, x_states (1 or n_states) volumes. T: host n_states x 6.
  * di=1 forward: out holds n_states volumes. di=0 inverse: out holds the sum
  * over states when sumR!=0, else n_states volumes. useFull: 1 full, 0
@@ -140,11 +158,16 @@ int disorder_precompute_factors(disorder_ctx ctx, disorder_plan plan, const floa
  * until exit. Limits: at most 256 states and at most 32 MiB of tables per call
  * (about 12 states at 256x256x176, about 200 at 64x64x44), rotations within
  * +-90 degrees, and di=0 (inverse) takes n_states volumes and writes them
- * back without summing. Larger requests fail with DISORDER_BAD_ARG. The first
- * call on a device resolves the array's device address (cudaGetSymbolAddress)
- * and should come before any stream capture. All calls share the one array:
- * calls that overlap on the GPU (other streams or threads) race with each
- * other. The plan must already exist (disorder_plan_create allocates). */
+ * back without summing. Larger requests fail with DISORDER_BAD_ARG. The
+ * array's device address is resolved when the context is created
+ * (disorder_ctx_create, cudaGetSymbolAddress), which loads the module holding
+ * it and commits its 32 MiB on that device then; the call itself allocates
+ * nothing and loads no data module (its kernels, shared with the other
+ * entry points, load on first use like any CUDA code unless
+ * CUDA_MODULE_LOADING=EAGER). All calls share the one array and each call
+ * rewrites the part it uses before reading it: calls that overlap on the GPU
+ * (other streams, contexts or host threads) race with each other. The plan
+ * must already exist (disorder_plan_create allocates). */
 int disorder_sinc_rigid_transform_static(disorder_ctx ctx, disorder_plan plan, const void* x,
                                          int32_t x_states, const float* T, int32_t n_states,
                                          int32_t di, int32_t useFull, void* out);
@@ -222,7 +245,7 @@ int disorder_resample(disorder_ctx ctx, const void* x, const int32_t* Nin, int32
                       const int32_t* Nout, void* out);
 
 /* Rows of a sample array picked for a pyramid level (the k-space crop of
- * Methods/downsampleOperators.m:53,67 on per-sample data):
+ * Methods/downsampleOperators.m:48-51 on per-sample data):
  * y_out[i + n_out*r] = scale * y_in[idx[i] + n_in*r], r < rows (readout x coils).
  * idx: device int32 n_out. */
 int disorder_gather_samples(disorder_ctx ctx, const void* y_in, int64_t n_in, int64_t rows,

@@ -14,7 +14,7 @@ Supported structure fields (the ones the aligned reconstruction sets):
 
 Two evaluation methods give the same operator:
   method="rows": the reference's literal per-sample DFT rows
-    (encode.m:120-136, decode.m:189-205, encodedecode.m:119-143), cost
+    (encode.m:120-136, decode.m:42-58, encodedecode.m:119-143), cost
     O(Ns*N1*N2*N3*C); small sizes only.
   method="fft": the separable full 2-D DFT plus gather/scatter of the same
     unitary DFT (DC-first rows of build1DFTM(N,1), buildHarmonicSampling.m:30,39).
@@ -125,7 +125,7 @@ def _sample_weights(EH, a, b):
 
 
 def _decode_states(y, E, EH, segs, method, apply_we=True):
-    """FOURIER DOMAIN (SEGMENTS) + COIL PROFILES of decode.m:189-232: per
+    """FOURIER DOMAIN (SEGMENTS) + COIL PROFILES of decode.m:42-58,78-85: per
     segment F^H of its samples, times conj(S), summed over coils."""
     S = E.Sf
     N1, N2, N3, C = S.shape
@@ -153,7 +153,7 @@ def _decode_states(y, E, EH, segs, method, apply_we=True):
 
 
 def _inverse_and_sum(xo, E, segs, dtype):
-    """RIGID TRANSFORM (MOTION STATES) of decode.m:243-260: inverse transform of
+    """RIGID TRANSFORM (MOTION STATES) of decode.m:95-113: inverse transform of
     the motion segments (sumR=0), then sum over all segments."""
     mot = [j for j, s in enumerate(segs) if s < E.NMs]
     if E.has("Tr") and _any_motion(E) and mot:

@@ -218,3 +218,37 @@ def LMsolver(y, E, x, C=None, method="fft", dtype=np.float64, deb=0):
     else:
         Eo = Enmin
     return E.copy(Tr=T.astype(np.float32), cT=cTFull, w=w, En=Eo, EnPrev=EnPrev)
+
+
+def alternating_reconstruction(y, E, n_outer=10, n_cg=3, n_lm=1, winit=1e-3, tL=(0.05, 0.02), reg=1e-9,
+                               on_stage=None, method="fft", dtype=np.float64):
+    """The fixed-schedule alignment at one resolution (the small simulation
+    case): n_outer times CGsolver (n_cg iterations, RelativeResidual2Error
+    with tolerance 0, from the current image, A.Se = 1/(sum_c |S_c|^2 + reg),
+    Reconstruction/solveXT.m:231-233,431), then n_lm LMsolver iterations
+    (solveXT.m:507), with the motion-convergence resets of solveXT.m:379-384.
+    E carries Sf, the sampling fields and the grids (E.Tr is ignored: motion
+    starts at zero). on_stage(stage, n, x, E) after every update. Returns (x, E)."""
+    S = int(E.NMs)
+    Se = 1.0 / (np.sum(np.abs(E.Sf) ** 2, axis=3) + reg)
+    A = enc.Struct(Se=Se)
+    E = E.copy(Tr=np.zeros((S, 6), np.float32), w=np.full(S, winit), cT=np.zeros(S, bool), winit=winit,
+               tL=list(tL))
+    Sf = E.Sf
+    x = None
+    nReset, cont = 0, 0
+    for n in range(n_outer):
+        if nReset == 0 or cont % nReset == 0 or np.all(E.cT):
+            nReset += 1
+            cont = 0
+            E = E.copy(cT=np.zeros(S, bool))
+        cont += 1
+        x, _, _ = CGsolver(y, E, None, A, None, None, x, n_cg, "RelativeResidual2Error", 0.0, method, dtype)
+        if on_stage:
+            on_stage("cg", n, x, E)
+        for _ in range(n_lm):
+            E = LMsolver(y, E.copy(Sf=Sf), x, method=method, dtype=dtype)
+        E = E.copy(Sf=Sf)
+        if on_stage:
+            on_stage("lm", n, x, E)
+    return x, E

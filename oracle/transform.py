@@ -1,7 +1,7 @@
 """Sinc-interpolated rigid transform, its factors and its gradient (oracle).
 
 TEST INFRASTRUCTURE ONLY. Restates
-  Methods/precomputeFactorsSincRigidTransform.m:24-249 (di, cg in {0,1}, gr=1, sh=1),
+  Methods/precomputeFactorsSincRigidTransform.m:24-133 (di, cg in {0,1}, gr=1, sh=1),
   Methods/sincRigidTransform.m:21-116,
   Methods/sincRigidTransformGradient.m:19-149,
   Methods/flipping.m:11-22, Methods/shifting.m:25-49,
@@ -62,7 +62,7 @@ class Factors:
 
 
 def precomputeFactorsSincRigidTransform(grids_, T, di=1, cg=0, dtype=np.float64, cGrid=None):
-    """Methods/precomputeFactorsSincRigidTransform.m:24-249 with gr=1, sh=1.
+    """Methods/precomputeFactorsSincRigidTransform.m:24-133 with gr=1, sh=1.
 
     Returns (et, etg) where et.e1[m], et.e2[m], et.e3[m] are the translation,
     tan-shear and sin-shear factors (et{1}{m}, et{2}{m}, et{3}{m}), et.flip[m]
@@ -77,23 +77,23 @@ def precomputeFactorsSincRigidTransform(grids_, T, di=1, cg=0, dtype=np.float64,
     S = T.shape[0]
     N = grids_.N
     if cGrid is None:
-        cGrid = [n / 2.0 + 1 for n in N]  # :147
+        cGrid = [n / 2.0 + 1 for n in N]  # :31
     Td = T.astype(rdt)
-    t = ((-1) ** di) * 1j * Td[:, 0:3]  # :161
-    theta = wrapToPi(Td[:, 3:6])  # :162
+    t = ((-1) ** di) * 1j * Td[:, 0:3]  # :45
+    theta = wrapToPi(Td[:, 3:6])  # :46
     et = Factors()
-    et.flip = [np.abs(theta[:, n]) > np.pi / 2 for n in range(3)]  # :164-166
-    et.cent = [{PER[0, n]: cGrid[PER[0, n]], PER[1, n]: cGrid[PER[1, n]]} for n in range(3)]  # :168
-    theta = wrapToPiHalf(theta)  # :170
-    tantheta2 = np.tan(theta / 2)  # :172-173
-    tantheta2j = ((-1) ** (di - 1)) * 1j * tantheta2  # :174
-    sintheta = ((-1) ** di) * 1j * np.sin(theta)  # :175-176
+    et.flip = [np.abs(theta[:, n]) > np.pi / 2 for n in range(3)]  # :48-51
+    et.cent = [{PER[0, n]: cGrid[PER[0, n]], PER[1, n]: cGrid[PER[1, n]]} for n in range(3)]  # :52
+    theta = wrapToPiHalf(theta)  # :54
+    tantheta2 = np.tan(theta / 2)  # :56-57
+    tantheta2j = ((-1) ** (di - 1)) * 1j * tantheta2  # :58
+    sintheta = ((-1) ** di) * 1j * np.sin(theta)  # :59-60
     if cg > 0:
-        tanthetacuad = (1 + tantheta2 * tantheta2) / 2  # :179-180
-        costheta = np.cos(theta)  # :181
+        tanthetacuad = (1 + tantheta2 * tantheta2) / 2  # :63-64
+        costheta = np.cos(theta)  # :65
     st = lambda v: along(v, 4)  # noqa: E731  states on axis 4
     et.e2, et.e3 = [], []
-    for m in range(3):  # :194-197
+    for m in range(3):  # :78-81
         rk1 = grids_.rk(1, m).astype(rdt)
         rk2 = grids_.rk(2, m).astype(rdt)
         et.e2.append(np.exp(st(tantheta2j[:, m]) * rk1).astype(cdt))
@@ -102,17 +102,17 @@ def precomputeFactorsSincRigidTransform(grids_, T, di=1, cg=0, dtype=np.float64,
     if cg > 0:
         etg = Factors()
         etg.e2, etg.e3 = [], []
-        for m in range(3):  # :204-218
+        for m in range(3):  # :88-102
             rk1 = grids_.rk(1, m).astype(rdt)
             rk2 = grids_.rk(2, m).astype(rdt)
             etg.e2.append((1j * st(tanthetacuad[:, m]) * rk1 * et.e2[m]).astype(cdt))
             etg.e3.append((-1j * st(costheta[:, m]) * rk2 * et.e3[m]).astype(cdt))
     et.e1 = []
-    for m in range(3):  # :230-231 (gr=1)
+    for m in range(3):  # :114-115 (gr=1)
         k = along(grids_.kGrid[m].astype(rdt), m)
         et.e1.append(np.exp(st(t[:, m]) * k).astype(cdt))
     if cg > 0:
-        etg.e1 = [(-1j * along(grids_.kGrid[m].astype(rdt), m)).astype(cdt) for m in range(3)]  # :236-240
+        etg.e1 = [(-1j * along(grids_.kGrid[m].astype(rdt), m)).astype(cdt) for m in range(3)]  # :120-125
     et.S = S
     et.N = N
     return et, etg
@@ -120,9 +120,9 @@ def precomputeFactorsSincRigidTransform(grids_, T, di=1, cg=0, dtype=np.float64,
 
 def shifting(x, H):
     """Methods/shifting.m:25-49 (f=0, zp=0) for complex x. H maps axis ->
-    scalar shift. Integer shifts are circular index shifts (:200-204);
+    scalar shift. Integer shifts are circular index shifts (:29-37);
     others are DFT phase ramps exp(-i*k*h) with k the ifftshifted grid
-    (2*pi/N)((1:N)-ceil((N+1)/2)) (:210-216)."""
+    (2*pi/N)((1:N)-ceil((N+1)/2)) (:38-47)."""
     for m, hh in sorted(H.items()):
         n = x.shape[m]
         if float(hh) == np.round(hh):
