@@ -36,7 +36,15 @@ CFG = dict(N=(256, 256, 176), coils=32, coils_kept=16, shots=64, rot_deg=5.0, tr
            ellipsoids=40, seed=2000)
 SMALL = dict(N=(64, 64, 48), coils=8, coils_kept=6, shots=16, rot_deg=5.0, trans_vox=3.0, snr_db=25.0,
              ellipsoids=12, seed=2001)
-NOMINAL_COUNTS = {"outer": [20, 20], "cg_final": 30}  # nominal schedule for the CPU reference estimate
+# The schedule the plain method runs on this seeded scan (outer CG + LM
+# iterations at the 64x64x44 and 128x128x88 levels, final CG iterations at full
+# size), as the GPU arm reports it in its `schedule` key. The reference arm
+# extrapolates its sampled CPU timings to this same schedule.
+PLAIN_SCHEDULE = {"outer": [9, 3], "cg_final": 7}
+# DRAM bytes (read + write) of one normal operator (encodedecode) at
+# 256x256x176, 16 coils, 64 shots: the sum over its 258 launches in the ncu
+# launch list (profiles/normal_operator_launches_256x256x176_64shots.md).
+TRAFFIC_NORMAL_OP = 656.2e9
 # DRAM bytes (read + write) per line-pass launch at 64 states: an ncu capture of
 # the contiguous (pipe_kernel) and strided (tma_kernel) passes at 4 states
 # (679.5 MB per launch, launches 2-4 of a forward transform) scaled by 16;
@@ -165,41 +173,20 @@ class NvmlClockSampler:
 
 
 # ---------------------------------------------------------------- scan synthesis
-def build_scan(ctx, cfg, use_torch=True):
-    """Synthesise the scan on the GPU: x_gt, 32 coils, shot map, motion and
-    noisy samples y = encode(x_gt) + noise (Simulation/synthesizeY.m:82-84)."""
+def build_scan(ctx, cfg):
+    """Synthesise the scan on the GPU with the library's generator kernels:
+    x_gt, the coil maps, shot map, motion and noisy samples
+    y = encode(x_gt) + noise (Simulation/synthesizeY.m:82-84)."""
     import disorder_b200 as db
-    from disorder_b200 import synth
+    from disorder_b200 import synth, synth_gpu
     N = tuple(cfg["N"])
     rng = np.random.default_rng(cfg["seed"])
     sc = synth.Scan()
     sc.N = N
-    if use_torch:
-        import torch
-        from disorder_b200 import synth_gpu
-        dev = "cuda:%d" % ctx.device
-        xt = synth_gpu.phantom_torch(N, cfg["ellipsoids"], rng, dev).to(torch.complex64)
-        St = synth_gpu.coils_torch(N, cfg["coils"], rng, dev=dev)
-        sigma = _sigma_torch(cfg["snr_db"], xt, St)
-        x_gt = ctx.empty(N)
-        S = ctx.empty(N + (cfg["coils"],))
-        xf = xt.permute(2, 1, 0).contiguous()
-        Sf = St.permute(3, 2, 1, 0).contiguous()
-        torch.cuda.synchronize()
-        ctx.check(ctx.lib.disorder_memcpy_d2d(ctx.h, x_gt.ptr, xf.data_ptr(), x_gt.nbytes))
-        ctx.check(ctx.lib.disorder_memcpy_d2d(ctx.h, S.ptr, Sf.data_ptr(), S.nbytes))
-        ctx.synchronize()
-        del xf, Sf, St
-        sc.x_gt_host = xt.cpu().numpy()
-        del xt
-    else:
-        xh = synth.phantom(N, cfg["ellipsoids"], rng)
-        xh = (xh / np.linalg.norm(xh.ravel())).astype(np.complex64)
-        Sh = synth.coil_maps(N, cfg["coils"], rng)
-        sigma = synth.snr_to_sigma(cfg["snr_db"], xh, Sh)
-        x_gt = ctx.upload(xh)
-        S = ctx.upload(Sh)
-        sc.x_gt_host = xh
+    x_gt = synth_gpu.phantom(ctx, N, cfg["ellipsoids"], rng)
+    S = synth_gpu.coil_maps(ctx, N, cfg["coils"], rng)
+    sigma = synth_gpu.snr_sigma(cfg["snr_db"], int(np.prod(N)))
+    sc.x_gt_host = x_gt.numpy()
     sc.H = synth.random_checkered(N[:2], cfg["shots"], rng)
     sc.ky, sc.kz, sc.nEc, sc.mSt, sc.iSt = synth.sample_lists(sc.H, cfg["shots"])
     sc.T_gt = synth.motion(cfg["shots"], cfg["rot_deg"], cfg["trans_vox"], rng)
@@ -208,34 +195,10 @@ def build_scan(ctx, cfg, use_torch=True):
     E = db.Struct(Tr=sc.T_gt, NMs=cfg["shots"], NSe=cfg["shots"] + 1, Sf=S, grids=db.generateTransformGrids(N, N, cent),
                   ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt)
     y = db.encode(x_gt, E, ctx=ctx)
-    if use_torch:
-        import torch
-        yt = torch.empty(y.nbytes // 8, dtype=torch.complex64, device="cuda:%d" % ctx.device)
-        ctx.check(ctx.lib.disorder_memcpy_d2d(ctx.h, yt.data_ptr(), y.ptr, y.nbytes))
-        ctx.synchronize()
-        g = torch.Generator(device=yt.device)
-        g.manual_seed(cfg["seed"] + 7919)
-        yt += sigma * torch.complex(torch.randn(yt.shape, generator=g, device=yt.device),
-                                    torch.randn(yt.shape, generator=g, device=yt.device))
-        torch.cuda.synchronize()
-        ctx.check(ctx.lib.disorder_memcpy_d2d(ctx.h, y.ptr, yt.data_ptr(), y.nbytes))
-        ctx.synchronize()
-        del yt
-    else:
-        yh = synth.add_noise(y.numpy(), sigma, cfg["seed"] + 7919)
-        y = ctx.upload(yh)
+    synth_gpu.add_noise(ctx, y, sigma, cfg["seed"] + 7919)
+    ctx.synchronize()
     sc.x_gt, sc.S, sc.y = x_gt, S, y
     return sc
-
-
-def _sigma_torch(snr_db, x, S):
-    """Simulation/SNRToLevels.m:23-33 on torch tensors, for the unitary
-    encoding (see disorder_b200.synth.snr_to_sigma)."""
-    import torch
-    meanS = torch.mean(torch.abs(x) ** 2).item()
-    meanN = meanS / (10 ** (snr_db / 10))
-    P = torch.mean(1.0 / (torch.sum(torch.abs(S) ** 2, dim=3) + 1e-3)).item()
-    return float(math.sqrt(meanN / (2 * P)))
 
 
 def nrmse(ctx, x, x_gt_host):
@@ -244,14 +207,17 @@ def nrmse(ctx, x, x_gt_host):
 
 
 # ---------------------------------------------------------------- CPU baseline (oracle, FP64)
-def cpu_estimate(N, n_states, C, counts, budget_note=True):
+def cpu_estimate(N, n_states, C, counts, ctx=None):
     """Time the FP64 NumPy restatement (oracle) on bounded samples of the
     workload and extrapolate to one reconstruction with the given schedule:
     counts = {"outer": [n_outer_L1, n_outer_L2], "cg_final": n}. Samples: the
     normal operator (encodedecode) for 8 of the 64 states at 64x64x44, the LM
     step for 8 states at 64x64x44, and the normal operator for 1 state at the
     full size; other levels and state counts are scaled by voxel count and
-    state count. Returns (seconds per reconstruction, threads, description)."""
+    state count. With a context, the library's forward transform, encode,
+    decode and encodedecode of that full-size state are checked against the
+    oracle's on the same inputs (relative L2 errors, FP32 against FP64).
+    Returns (seconds per reconstruction, threads, description, errors)."""
     from disorder_b200 import synth
     from oracle import encoding as oenc
     from oracle import grids as og
@@ -288,7 +254,7 @@ def cpu_estimate(N, n_states, C, counts, budget_note=True):
     t_lm1 = (time.perf_counter() - t0) * n_states / sub
     x3, E3 = problem(tuple(N), 1, 3)
     t0 = time.perf_counter()
-    oenc.encodedecode(x3, E3, None)
+    ed3 = oenc.encodedecode(x3, E3, None)
     t_ed3 = (time.perf_counter() - t0) * n_states
     v1, v2, v3 = np.prod(L1), np.prod(L2), np.prod(N)
     t_ed2, t_lm2 = t_ed1 * v2 / v1, t_lm1 * v2 / v1
@@ -299,11 +265,57 @@ def cpu_estimate(N, n_states, C, counts, budget_note=True):
             "at %s, encodedecode 1/%d states at %s; extrapolated by state count and voxel count to the schedule "
             "%s" % (threads, n_states, "x".join(map(str, L1)), n_states, "x".join(map(str, L1)), n_states,
                     "x".join(map(str, N)), json.dumps(counts)))
-    return est, threads, desc
+    errs = oracle_check(ctx, x3, E3, ed3) if ctx is not None else None
+    return est, threads, desc, errs
+
+
+def oracle_check(ctx, x, Eo, ed_oracle):
+    """Relative L2 error of the library (FP32 on the GPU) against the FP64
+    oracle for one motion state at full size: forward transform, encode,
+    decode and encodedecode of the same inputs (state 0 of the sampled
+    problem, its samples only)."""
+    import disorder_b200 as db
+    from oracle import encoding as oenc
+    from oracle.transform import precomputeFactorsSincRigidTransform as opf
+    from oracle.transform import sincRigidTransform as ost
+    N = tuple(x.shape)
+    n0, n1 = int(Eo.nEc[0]), int(Eo.nEc[1])
+    T = np.asarray(Eo.Tr[:1], np.float32)
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    Ed = db.Struct(Tr=T, NMs=1, NSe=1, Sf=ctx.upload(Eo.Sf.astype(np.complex64)),
+                   grids=db.generateTransformGrids(N, N, cent), ky=Eo.ky[n0:n1], kz=Eo.kz[n0:n1],
+                   nEc=np.array([0, n1 - n0], np.int64), mSt=np.zeros(n1 - n0, np.int32))
+    Es = Eo.copy(Tr=T, NMs=1, NSe=1, ky=Eo.ky[n0:n1], kz=Eo.kz[n0:n1], nEc=np.array([0, n1 - n0]), vA=None,
+                 mSt=np.zeros(n1 - n0, np.int32))
+    x32 = x.astype(np.complex64)
+
+    def rel(a, b):
+        return float(np.linalg.norm((np.asarray(a) - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    out = {"workload": "%s, %d coils, 1 state of %d samples" % ("x".join(map(str, N)), Eo.Sf.shape[3], n1 - n0)}
+    et, _ = db.precomputeFactorsSincRigidTransform(Ed.grids, T, 1)
+    zt, _ = db.sincRigidTransform(x32, et, 1, ctx=ctx)
+    oet, _ = opf(Eo.grids, T, 1, 0)
+    out["transform"] = rel(zt[..., 0], ost(x.reshape(N + (1, 1)), oet, 1)[:, :, :, 0, 0])
+    yo = oenc.encode(x, Es)
+    out["encode"] = rel(db.encode(x32, Ed, ctx=ctx), yo)
+    out["decode"] = rel(db.decode(yo.astype(np.complex64), None, Ed, ctx=ctx), oenc.decode(yo, None, Es))
+    out["encodedecode"] = rel(db.encodedecode(x32, Ed, None, ctx=ctx), ed_oracle)
+    return out
+
+
+def alg_bytes_normal_op(N, C, S, Ns):
+    """Algorithmic bytes of one normal operator (encodedecode) over S motion
+    states: per state and direction 10 volume passes of 16 bytes per voxel, one
+    read of the volume and of the C coil maps, and the state's Ns x N3 x C
+    samples; the adjoint adds the state accumulation (16 bytes per voxel)."""
+    V = float(np.prod(N))
+    per_dir = 16 * V * 10 + 8 * V + 8 * V * C + 8 * Ns * N[2] * C
+    return S * (2 * per_dir + 16 * V)
 
 
 # ---------------------------------------------------------------- transform only
-def transform_only(cfg, S, warmup, steps):
+def transform_only(cfg, S, warmup, steps, precision="fp32"):
     """Time the forward transform, the inverse without and with the state sum
     of a random volume of the scan size with S random motion states, through
     the C ABI with preallocated buffers (CUDA events, best of `steps` after
@@ -314,6 +326,7 @@ def transform_only(cfg, S, warmup, steps):
     N = tuple(cfg["N"])
     rng = np.random.default_rng(0)
     ctx = db.Context(0)
+    ctx.set_precision(precision)
     x = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
     T = synth.motion(S, cfg["rot_deg"], cfg["trans_vox"], rng)
     cent = [math.ceil((n + 1) / 2.0) for n in N]
@@ -344,11 +357,12 @@ def transform_only(cfg, S, warmup, steps):
             ts.append(ctx.elapsed_ms(0, 1))
         t = min(ts)
         res[name] = {"ms": t, "GB/s": 11 * 16.0 * V * S / (t * 1e-3) / 1e9}
-    print(json.dumps({"transform": "x".join(map(str, N)), "states": S, "launches": ctx.launches, "results": res}))
+    print(json.dumps({"transform": "x".join(map(str, N)), "states": S, "precision": precision,
+                      "launches": ctx.launches, "results": res}))
 
 
 # ---------------------------------------------------------------- operators only
-def operator_only(cfg, S, warmup, steps, profile_region=False):
+def operator_only(cfg, S, warmup, steps, profile_region=False, precision="fp32"):
     """Time encode, decode and encodedecode (the normal operator) of a random
     volume of the scan size with the kept coil count, a random-checkered
     sampling of S shots and S random motion states, through the C ABI with
@@ -360,6 +374,7 @@ def operator_only(cfg, S, warmup, steps, profile_region=False):
     C = cfg["coils_kept"]
     rng = np.random.default_rng(1)
     ctx = db.Context(0)
+    ctx.set_precision(precision)
     x = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
     Sf = np.empty(N + (C,), np.complex64)
     for c in range(C):
@@ -404,8 +419,8 @@ def operator_only(cfg, S, warmup, steps, profile_region=False):
         ctx.check(calls["encodedecode"]())
         ctx.synchronize()
         torch.cuda.profiler.stop()
-    print(json.dumps({"operators": "x".join(map(str, N)), "coils": C, "shots": S, "launches": ctx.launches,
-                      "results": res}))
+    print(json.dumps({"operators": "x".join(map(str, N)), "coils": C, "shots": S, "precision": precision,
+                      "launches": ctx.launches, "results": res}))
 
 
 def phase_split(log):
@@ -419,35 +434,166 @@ def phase_split(log):
     return phases
 
 
-def learned_arm(ctx, sc, cfg, one_plain_s, counts=None):
-    """One reconstruction with the learned proposal (after one untimed warm-up
-    run): seconds, NRMSE, motion error, outer iterations, proposals kept and
-    LM state-steps, beside the plain method's."""
+def variant_arm(ctx, sc, cfg, plain_s, plain_nrmse, learned=False, precision="fp32"):
+    """One reconstruction of the scan with the learned proposal and / or the
+    tensor-core (mixed-precision) DFT passes and Gram (after one untimed
+    warm-up run): seconds (CUDA events), NRMSE, whether it reaches the plain
+    method's NRMSE within 1%, motion error, outer iterations, proposals kept
+    and LM state-steps."""
     from disorder_b200 import proposal, recon
-    if not os.path.exists(proposal.WEIGHTS):
-        return {"unavailable": "no trained proposal weights at %s" % os.path.relpath(proposal.WEIGHTS, ROOT)}
-    net = proposal.MotionNet.load(ctx, proposal.WEIGHTS)
+    net = None
+    if learned:
+        if not os.path.exists(proposal.WEIGHTS):
+            return {"unavailable": "no trained proposal weights at %s" % os.path.relpath(proposal.WEIGHTS, ROOT)}
+        net = proposal.MotionNet.load(ctx, proposal.WEIGHTS)
 
     def run():
         return recon.aligned_reconstruction(ctx, sc.S, sc.y, sc.H, cfg["shots"], cfg["N"], perc=cfg["coils_kept"],
                                             proposal=net)
 
-    run()
-    ctx.synchronize()
-    ctx.event(10)
-    x, T, log = run()
-    ctx.event(11)
-    t = ctx.elapsed_ms(10, 11) * 1e-3
+    ctx.set_precision(precision)
+    try:
+        run()
+        ctx.synchronize()
+        ctx.event(10)
+        x, T, log = run()
+        ctx.event(11)
+        t = ctx.elapsed_ms(10, 11) * 1e-3
+    finally:
+        ctx.set_precision("fp32")
     ev = log.events
     d = np.asarray(T, float) - np.asarray(sc.T_gt, float)
-    return {"value": t, "unit": "s", "vs_plain": t / one_plain_s, "nrmse": nrmse(ctx, x, sc.x_gt_host),
+    e = nrmse(ctx, x, sc.x_gt_host)
+    return {"value": t, "unit": "s", "vs_plain": t / plain_s, "nrmse": e,
+            "reaches_plain_nrmse": bool(e <= 1.01 * plain_nrmse), "precision": precision, "learned": learned,
             "motion_max_err": {"trans_vox": float(np.max(np.abs(d[:, :3]))),
                                "rot_deg": float(np.degrees(np.max(np.abs(d[:, 3:]))))},
             "outer": [sum(1 for e in ev if e["step"] == "lm" and e["level"] == lv) for lv in (0, 1)],
+            "cg_final": sum(e["iters"] for e in ev if e["step"] == "cg" and e["level"] == 2),
             "proposals_kept": sum(e["accepted"] for e in ev if e["step"] == "proposal"),
             "lm_state_steps": [sum(e["lm_states"] for e in ev if e["step"] == "lm" and e["level"] == lv)
                                for lv in (0, 1)],
             "phases_s": {k: round(v, 4) for k, v in phase_split(log).items()}}
+
+
+# ---------------------------------------------------------------- batched uneven scans
+def batch_arm(n_scans=32, seed=4000, workers=(1, 2, 4)):
+    """32 independent synthetic scans with per-axis sizes from
+    {96,128,160,192,256}, coils from {8,16,32} and shots from {16,32,64,96}
+    (motion U(-5,5) deg / voxels, 25 dB), reconstructed on this GPU by the
+    batched executor (disorder_b200.batch) after its autotuner picked the
+    worker count and strided-pass engine on the costliest scans. Reports
+    scans/s, p50 / p99 per-scan seconds and the NRMSE spread."""
+    from disorder_b200 import batch
+    specs = batch.uneven_specs(n_scans, seed)
+    runner = batch.BatchRunner(workers=max(workers))
+    t0 = time.perf_counter()
+    scans = [batch.build(runner.ctxs[0], sp) for sp in specs]
+    t_build = time.perf_counter() - t0
+    best, trials = batch.tune(runner, scans, worker_counts=workers)
+    r = runner.run(scans, workers=best["workers"])
+    e = [v for v in r["nrmse"] if v is not None]
+    out = {"value": r["scans_per_s"], "unit": "scans/s", "scans": n_scans, "p50_s": r["p50_s"], "p99_s": r["p99_s"],
+           "wall_s": r["wall_s"], "workers": best["workers"], "tma": best["tma"], "tuning": trials,
+           "build_s": t_build, "failures": r["failures"],
+           "nrmse": {"min": min(e), "median": float(np.median(e)), "max": max(e)} if e else None,
+           "workload": "%d scans: sizes %s, coils %s, shots %s" % (
+               n_scans, sorted({s for sp in specs for s in sp["N"]}), sorted({sp["coils"] for sp in specs}),
+               sorted({sp["shots"] for sp in specs}))}
+    del scans, runner
+    return out
+
+
+# ---------------------------------------------------------------- rooflines
+def normal_operator_roofline(ctx, cfg, peak, pkind, reps=5):
+    """One normal operator (encodedecode) of a random volume of the scan size
+    with the kept coil count and all shots (random-checkered sampling, random
+    motion) through the C ABI with preallocated buffers; CUDA events on the
+    library's stream, mean of `reps` after one warm-up call. achieved =
+    algorithmic bytes (alg_bytes_normal_op) / time."""
+    import disorder_b200 as db
+    from disorder_b200 import _lib, api, synth
+    N = tuple(cfg["N"])
+    C, S = cfg["coils_kept"], cfg["shots"]
+    rng = np.random.default_rng(11)
+    Sd = ctx.empty(N + (C,))
+    for c in range(C):
+        v = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+        ctx.check(ctx.lib.disorder_memcpy_h2d(ctx.h, Sd.ptr + c * v.nbytes, v.ctypes.data, v.nbytes))
+    H = synth.random_checkered(N[:2], S, rng)
+    ky, kz, nEc, mSt, _ = synth.sample_lists(H, S)
+    T = synth.motion(S, cfg["rot_deg"], cfg["trans_vox"], rng)
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    E = db.Struct(Tr=T, NMs=S, NSe=S + 1, Sf=Sd, grids=db.generateTransformGrids(N, N, cent), ky=ky, kz=kz,
+                  nEc=nEc, mSt=mSt)
+    plan = api._plan(E, ctx)
+    xd = ctx.upload((rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64))
+    out = ctx.empty(N)
+    Tf = np.asfortranarray(np.asarray(T, np.float32))
+    Tp = Tf.ctypes.data_as(_lib.FP)
+
+    def call():
+        ctx.check(ctx.lib.disorder_encodedecode(ctx.h, plan.h, xd.ptr, Sd.ptr, C, Tp, None, out.ptr))
+
+    call()
+    ctx.synchronize()
+    ctx.event(4)
+    for _ in range(reps):
+        call()
+    ctx.event(5)
+    t = ctx.elapsed_ms(4, 5) / reps
+    Ns = int(np.max(np.diff(nEc)[:S]))
+    alg = alg_bytes_normal_op(N, C, S, Ns)
+    achieved = alg / (t * 1e-3) / 1e9
+    del Sd, xd, out
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": TRAFFIC_NORMAL_OP, "peak_kind": pkind, "bytes_per_launch": alg, "ms": t,
+            "kernel": "normal operator encodedecode (transform line passes, coil expand, weighted dim-2 pass, "
+                      "coil combine, inverse transform with state sum)",
+            "timing": "one encodedecode of %s, %d coils, %d shots through the C ABI, CUDA events, mean of %d; "
+                      "achieved = algorithmic bytes (10 volume passes per state and direction, one read of the "
+                      "volume, coil maps and samples, state accumulation) / time; traffic = ncu DRAM bytes summed "
+                      "over the operator's launches" % ("x".join(map(str, N)), C, S, reps)}
+
+
+def transform_roofline(ctx, cfg, sc, peak, pkind, reps=5):
+    """The transform's line passes at full size: one forward transform of the
+    64 states (11 launches: pipe_kernel for the dim-1 passes and tma_kernel for
+    the dim-2 and dim-3 passes, each reading and writing the 64 complex64
+    state volumes), CUDA events, mean of `reps`."""
+    import disorder_b200 as db
+    from disorder_b200 import _lib, api
+    N = cfg["N"]
+    V = int(np.prod(N))
+    S = cfg["shots"]
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    grids = db.generateTransformGrids(N, N, cent)
+    et, _ = db.precomputeFactorsSincRigidTransform(grids, sc.T_gt, 1)
+    tplan = api._transform_plan(ctx, grids)
+    Tf = np.asfortranarray(et.T.astype(np.float32))
+    Tp = Tf.ctypes.data_as(_lib.FP)
+    xg = ctx.upload(sc.x_gt_host.astype(np.complex64))
+    outt = ctx.empty(tuple(N) + (S,))
+
+    def fwd():
+        ctx.check(ctx.lib.disorder_sinc_rigid_transform(ctx.h, tplan.h, xg.ptr, 1, Tp, S, 1, 1, 1, outt.ptr))
+
+    fwd()
+    ctx.synchronize()
+    ctx.event(4)
+    for _ in range(reps):
+        fwd()
+    ctx.event(5)
+    t_fwd = ctx.elapsed_ms(4, 5) / reps
+    del outt, xg
+    n_pass = 11
+    bytes_per_launch = 16.0 * V * S
+    achieved = bytes_per_launch / (t_fwd / n_pass * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": TRAFFIC_PER_LAUNCH, "peak_kind": pkind, "bytes_per_launch": bytes_per_launch,
+            "kernel": "fp::pipe_kernel (dim-1 passes) + fp::tma_kernel (dim-2/3 passes): sinc-transform line passes",
+            "timing": "one forward transform (11 launches, phase-seed build included) through the C ABI, "
+                      "%d states, CUDA events, mean of %d" % (S, reps)}
 
 
 # ---------------------------------------------------------------- ranks
@@ -486,7 +632,11 @@ def main():
                     help="only time the sinc rigid transform of the scan size with STATES states")
     ap.add_argument("--operator-only", type=int, default=0, metavar="SHOTS",
                     help="only time encode / decode / encodedecode of the scan size with SHOTS shots")
-    ap.add_argument("--no-learned", action="store_true", help="skip the reconstruction with the learned proposal")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned / mixed-precision reconstructions")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch of uneven scans")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16x3", "tf32x3"],
+                    help="tensor-core contractions for --transform-only / --operator-only")
+    ap.add_argument("--batch-only", action="store_true", help="only run the batch of uneven scans")
     args = ap.parse_args()
     # grow the library's device pool once, when the context is created, instead
     # of mid-run: allocations of varying sizes otherwise map new memory at
@@ -494,9 +644,13 @@ def main():
     os.environ.setdefault("DISORDER_POOL_RESERVE_GB", "80")
     cfg = SMALL if args.small else CFG
     if args.transform_only:
-        return transform_only(cfg, args.transform_only, args.warmup, args.steps)
+        return transform_only(cfg, args.transform_only, args.warmup, args.steps, args.precision)
     if args.operator_only:
-        return operator_only(cfg, args.operator_only, args.warmup, args.steps, args.profile_region)
+        return operator_only(cfg, args.operator_only, args.warmup, args.steps, args.profile_region, args.precision)
+    if args.batch_only:
+        os.environ.setdefault("DISORDER_WORKSPACE_GB", "12")
+        print(json.dumps({"batch": batch_arm()}))
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -510,7 +664,7 @@ def main():
             return
         vals = []
         for it in range(args.warmup + args.steps):
-            est, thr, desc = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], NOMINAL_COUNTS)
+            est, thr, desc, _ = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], PLAIN_SCHEDULE)
             if it >= args.warmup:
                 vals.append(est)
         v = float(np.mean(vals))
@@ -532,7 +686,7 @@ def main():
     ctx = db.Context(local)
     cfg_r = dict(cfg)
     cfg_r["seed"] = replica_seed(cfg["seed"], rank)
-    sc = build_scan(ctx, cfg_r, use_torch=True)
+    sc = build_scan(ctx, cfg_r)
 
     def one(S, y):
         return recon.aligned_reconstruction(ctx, S, y, sc.H, cfg["shots"], cfg["N"], perc=cfg["coils_kept"])
@@ -611,46 +765,19 @@ def main():
 
     # the same reconstruction with the learned motion proposal at the coarsest
     # level (trained weights shipped with the package)
-    learned = learned_arm(ctx, sc, cfg, one_plain_s=ms * 1e-3, counts=None) if not args.no_learned else None
+    # the same reconstruction with the learned motion proposal, with the
+    # tensor-core DFT passes and Gram (BF16x3), and with both
+    variants = {}
+    if not args.no_learned:
+        for name, lrn, prec in (("learned", True, "fp32"), ("mixed", False, "bf16x3"),
+                                ("learned_mixed", True, "bf16x3")):
+            variants[name] = variant_arm(ctx, sc, cfg, ms * 1e-3, err, learned=lrn, precision=prec)
 
-    # roofline of the dominant kernel family: the line passes of the sinc rigid
-    # transform at full size (11 passes per forward transform, each reading
-    # and writing the 64 state volumes)
-    N = cfg["N"]
-    V = int(np.prod(N))
-    S = cfg["shots"]
-    cent = [math.ceil((n + 1) / 2.0) for n in N]
-    grids = db.generateTransformGrids(N, N, cent)
-    et, _ = db.precomputeFactorsSincRigidTransform(grids, sc.T_gt, 1)
-    from disorder_b200 import _lib, api
-    tplan = api._transform_plan(ctx, grids)
-    Tf = np.asfortranarray(et.T.astype(np.float32))
-    Tp = Tf.ctypes.data_as(_lib.FP)
-    xg = ctx.upload(sc.x_gt_host.astype(np.complex64))
-    outt = ctx.empty(tuple(N) + (S,))
-
-    def fwd():
-        ctx.check(ctx.lib.disorder_sinc_rigid_transform(ctx.h, tplan.h, xg.ptr, 1, Tp, S, 1, 1, 1, outt.ptr))
-
-    fwd()
-    ctx.synchronize()
-    reps = 5
-    ctx.event(4)
-    for _ in range(reps):
-        fwd()
-    ctx.event(5)
-    t_fwd = ctx.elapsed_ms(4, 5) / reps
-    del outt, xg
-    n_pass = 11
-    bytes_per_launch = 16.0 * V * S  # read + write of the 64 complex64 state volumes
-    achieved = bytes_per_launch / (t_fwd / n_pass * 1e-3) / 1e9
+    # roofline of the north star's unit, the normal operator (encodedecode) at
+    # full size, on its algorithmic bytes; the transform's line passes beside it
     peak, pkind = peaks()
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": TRAFFIC_PER_LAUNCH,
-            "kernel": "fp::pipe_kernel (dim-1 passes) + fp::tma_kernel (dim-2/3 passes): sinc-transform line passes",
-            "peak_kind": pkind, "bytes_per_launch": bytes_per_launch,
-            "timing": "one forward transform (11 launches, phase-seed build included) through the C ABI, "
-                      "%d states, CUDA events, mean of %d" % (S, reps)}
+    roof = normal_operator_roofline(ctx, cfg, peak, pkind)
+    roof_t = transform_roofline(ctx, cfg, sc, peak, pkind)
 
     out = {"metric": METRIC, "value": ms * 1e-3 / world, "unit": "s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
@@ -661,12 +788,17 @@ def main():
            "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": int(Sh.nbytes + yh.nbytes),
                    "d2h_bytes_per_step": int(V * 8), "parts": {k: round(v, 4) for k, v in e2e_parts.items()},
                    "phases_s": {k: round(v, 4) for k, v in e2e_phases.items()}, "clocks": e2e_clocks},
-           "roofline": roof}
-    if learned is not None:
-        out["learned"] = learned
+           "roofline": roof, "roofline_transform": roof_t}
+    out.update(variants)
+    if rank == 0 and not args.no_batch:
+        # free the benchmark scan first: the batch holds about 45 GB of scans
+        del sc
+        os.environ["DISORDER_WORKSPACE_GB"] = "12"
+        out["batch"] = batch_arm()
     if rank == 0 and not args.no_cpu:
-        est, thr, desc = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], counts)
+        est, thr, desc, errs = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], counts, ctx=ctx)
         out["cpu_baseline"] = {"value": est, "unit": "s", "cores": thr, "kind": "port", "sample": desc}
+        out["oracle_rel_err"] = errs
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -57,6 +57,8 @@ SIGNATURES = [
     ("disorder_kernel_launches", C.c_int64, [VP]),
     ("disorder_workspace_bytes", C.c_int64, [VP]),
     ("disorder_ctx_inject_fault", C.c_int, [VP, I32]),
+    ("disorder_ctx_set_precision", C.c_int, [VP, I32]),
+    ("disorder_ctx_set_tuning", C.c_int, [VP, I32, I32]),
     ("disorder_event_record", C.c_int, [VP, I32]),
     ("disorder_event_elapsed", C.c_int, [VP, I32, I32, FP]),
     ("disorder_plan_create", C.c_int, [VP, C.POINTER(GridDesc), C.POINTER(SamplingDesc), C.POINTER(VP)]),
@@ -84,6 +86,9 @@ SIGNATURES = [
     ("disorder_sample_energies", C.c_int, [VP, VP, VP, VP, I32, VP, FP, VP, DP]),
     ("disorder_residual_energies", C.c_int, [VP, VP, VP, I32, VP, DP]),
     ("disorder_backproject_states", C.c_int, [VP, VP, VP, VP, I32, VP, FP, I32, I32, VP]),
+    ("disorder_synth_phantom", C.c_int, [VP, C.POINTER(I32), I32, FP, I32, FP, I32, VP]),
+    ("disorder_synth_coils", C.c_int, [VP, C.POINTER(I32), I32, FP, C.c_float, VP]),
+    ("disorder_add_noise", C.c_int, [VP, VP, C.c_int64, C.c_float, C.c_uint64]),
     ("disorder_net_param_count", C.c_int64, []),
     ("disorder_net_create", C.c_int, [VP, C.POINTER(I32), I32, C.POINTER(VP)]),
     ("disorder_net_destroy", C.c_int, [VP]),

@@ -70,6 +70,15 @@ class Context:
     def synchronize(self):
         self.check(self.lib.disorder_synchronize(self.h))
 
+    PRECISIONS = {"fp32": 0, "bf16x3": 1, "tf32x3": 2}
+
+    def set_precision(self, mode):
+        """Arithmetic of the tensor-core contractions (disorder_ctx_set_precision):
+        'fp32' (CUDA cores), 'bf16x3' or 'tf32x3' (tcgen05, split operands)."""
+        self.check(self.lib.disorder_ctx_set_precision(self.h, self.PRECISIONS[mode] if isinstance(mode, str)
+                                                       else int(mode)))
+        self.precision = mode
+
     @property
     def launches(self):
         return int(self.lib.disorder_kernel_launches(self.h))

@@ -279,6 +279,26 @@ int disorder_ctx_inject_fault(disorder_ctx ctx, int32_t fault) {
   return DISORDER_OK;
 }
 
+int disorder_ctx_set_precision(disorder_ctx ctx, int32_t mode) {
+  CTX_CHECK(ctx);
+  if (mode < DISORDER_PRECISION_FP32 || mode > DISORDER_PRECISION_TF32X3)
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "set_precision: unknown mode %d", mode);
+  ctx->precision = mode;
+  return DISORDER_OK;
+}
+
+int disorder_ctx_set_tuning(disorder_ctx ctx, int32_t key, int32_t value) {
+  CTX_CHECK(ctx);
+  switch (key) {
+    case DISORDER_TUNE_TMA:
+      if (value != 0 && value != 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "set_tuning: TMA is 0 or 1");
+      ctx->tune_tma = value;
+      return DISORDER_OK;
+    default:
+      return dis_set_error(ctx, DISORDER_BAD_ARG, "set_tuning: unknown key %d", key);
+  }
+}
+
 int64_t disorder_workspace_bytes(disorder_ctx ctx) {
   return ctx ? (int64_t)(ctx->ws_bytes + ctx->ws2_bytes + ctx->small_bytes) : -1;
 }

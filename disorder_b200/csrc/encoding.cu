@@ -65,6 +65,38 @@ static size_t coil_slot_bytes(const disorder_plan_s* plan, int C, int N3c) {
   return (size_t)C * plan->N[0] * plan->N[1] * N3c * sizeof(float2);
 }
 
+// most samples of any of the segments
+static int max_samples(const disorder_plan_s* plan, const std::vector<int>& segs);
+
+// The coil stage of a call: the sample-sum stage (sumcoil.cu) when it has a
+// kernel for the sizes and its partial sums per slot are no larger than the
+// three-pass stage's per-coil volumes (at most N1 x lines-per-CTA samples per
+// segment), else the three passes. ldp: the partial sums' sample stride.
+struct CoilPlan {
+  bool sum = false;
+  int ldp = 0;
+  size_t per_slot = 0;  // coil-stage workspace bytes per slot
+};
+static CoilPlan coil_plan(const disorder_plan_s* plan, int C, int N3c, const std::vector<int>& segs) {
+  CoilPlan p;
+  p.per_slot = coil_slot_bytes(plan, C, N3c);
+  if (!dis_sum_coil_usable(plan)) return p;
+  const int ldp = std::max(1, max_samples(plan, segs));
+  const size_t pb = dis_sum_part_bytes(plan, C, N3c, ldp);
+  if (pb > p.per_slot) return p;
+  p.sum = true;
+  p.ldp = ldp;
+  p.per_slot = pb;
+  return p;
+}
+
+// slots per chunk for a coil stage of coil bytes per slot and extra bytes per slot
+static int chunk_for(const disorder_plan_s* plan, size_t coil, size_t extra, int n_total) {
+  const size_t per = coil + extra + dis_table_bytes(plan, 1, true);
+  const int ch = (int)std::max<size_t>(1, dis_budget_bytes() / std::max<size_t>(per, 1));
+  return std::max(1, std::min(ch, n_total));
+}
+
 int dis_chunk_slots(const disorder_plan_s* plan, int C, int N3c, size_t extra_per_slot, int n_total) {
   const size_t per = coil_slot_bytes(plan, C, N3c) + extra_per_slot + dis_table_bytes(plan, 1, true);
   size_t budget = dis_budget_bytes();
@@ -227,8 +259,9 @@ int dis_encode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
     }
     return DISORDER_OK;
   }
-  const int ch = dis_chunk_slots(plan, sp.C, sp.N3c, motion ? V * sizeof(float2) : 0, nsg);
-  const size_t need = (size_t)ch * coil_slot_bytes(plan, sp.C, sp.N3c) + (motion ? (size_t)ch * V * sizeof(float2) : 0) +
+  const CoilPlan cp = coil_plan(plan, sp.C, sp.N3c, sp.segs);
+  const int ch = chunk_for(plan, cp.per_slot, motion ? V * sizeof(float2) : 0, nsg);
+  const size_t need = (size_t)ch * cp.per_slot + (motion ? (size_t)ch * V * sizeof(float2) : 0) +
                       dis_table_bytes(plan, ch, false) + 4096 * 4;
   Workspace ws;
   DIS_TRY(dis_workspace(ctx, need, &ws));
@@ -238,16 +271,21 @@ int dis_encode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
     std::vector<int> segs(sp.segs.begin() + c0, sp.segs.begin() + c0 + n);
     int* d_seg = nullptr;
     DIS_TRY(dis_upload_ints(ctx, &w, segs, &d_seg));
-    float2* A = w.take<float2>((size_t)n * sp.C * plan->N[0] * plan->N[1] * sp.N3c);
+    float2* A = w.take<float2>((size_t)n * cp.per_slot / sizeof(float2));
     if (!A) return dis_set_error(ctx, DISORDER_OOM, "encode: workspace too small");
     const float2* z;
     long long Vz;
     int nm;
     DIS_TRY(states_of(ctx, plan, sp.x, sp.T, sp.T_n, motion, segs, &w, &z, &Vz, nullptr, &nm));
     CoilArgs ca = coil_args(plan, sp.Sf, sp.C, sp.n3_lo, sp.N3c, Vz, n, d_seg);
-    DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, z + (long long)sp.n3_lo * plan->N[0] * plan->N[1], A));
     const float scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
-    DIS_TRY(dis_coil_fft2_gather(ctx, plan, ca, A, y, sp.y_ld, sp.y_n3off, sp.y_N3, y_meas, scale));
+    const float2* z3 = z + (long long)sp.n3_lo * plan->N[0] * plan->N[1];
+    if (cp.sum) {
+      DIS_TRY(dis_coil_sum_fwd(ctx, plan, ca, z3, A, cp.ldp, y, sp.y_ld, sp.y_n3off, sp.y_N3, y_meas, scale));
+    } else {
+      DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, z3, A));
+      DIS_TRY(dis_coil_fft2_gather(ctx, plan, ca, A, y, sp.y_ld, sp.y_n3off, sp.y_N3, y_meas, scale));
+    }
   }
   return DISORDER_OK;
 }
@@ -262,8 +300,13 @@ int dis_encode_volumes(disorder_ctx_s* ctx, const disorder_plan_s* plan, const f
                      max_samples(plan, segs), y, y_meas, y_ld, y_n3off, y_N3, nullptr, nullptr);
   if (!A) return dis_set_error(ctx, DISORDER_OOM, "encode_volumes: no coil buffer");
   CoilArgs ca = coil_args(plan, Sf, C, n3_lo, N3c, plan->V, n, d_segs);
-  DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, vols + (long long)n3_lo * plan->N[0] * plan->N[1], A));
   const float scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
+  const float2* v3 = vols + (long long)n3_lo * plan->N[0] * plan->N[1];
+  // A holds the three-pass stage's per-coil volumes; the sample-sum stage's
+  // partial sums are never larger (coil_plan)
+  const CoilPlan cp = coil_plan(plan, C, N3c, segs);
+  if (cp.sum) return dis_coil_sum_fwd(ctx, plan, ca, v3, A, cp.ldp, y, y_ld, y_n3off, y_N3, y_meas, scale);
+  DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, v3, A));
   return dis_coil_fft2_gather(ctx, plan, ca, A, y, y_ld, y_n3off, y_N3, y_meas, scale);
 }
 
@@ -300,9 +343,10 @@ int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
     }
     return DISORDER_OK;
   }
-  const int ch = dis_chunk_slots(plan, sp.C, N3, V * sizeof(float2), nsg);
-  const size_t need = (size_t)ch * (coil_slot_bytes(plan, sp.C, N3) + V * sizeof(float2)) +
-                      dis_table_bytes(plan, ch, false) + 4096 * 4;
+  const CoilPlan cp = coil_plan(plan, sp.C, N3, sp.segs);
+  const size_t coil = cp.sum ? 0 : cp.per_slot;  // the adjoint sample-sum stage needs no buffer
+  const int ch = chunk_for(plan, coil, V * sizeof(float2), nsg);
+  const size_t need = (size_t)ch * (coil + V * sizeof(float2)) + dis_table_bytes(plan, ch, false) + 4096 * 4;
   Workspace ws;
   DIS_TRY(dis_workspace(ctx, need, &ws));
   for (int c0 = 0; c0 < nsg; c0 += ch) {
@@ -311,13 +355,17 @@ int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
     std::vector<int> segs(sp.segs.begin() + c0, sp.segs.begin() + c0 + n);
     int* d_seg = nullptr;
     DIS_TRY(dis_upload_ints(ctx, &w, segs, &d_seg));
-    float2* A = w.take<float2>((size_t)n * sp.C * V);
+    float2* A = cp.sum ? nullptr : w.take<float2>((size_t)n * sp.C * V);
     float2* U = w.take<float2>((size_t)n * V);
-    if (!A || !U) return dis_set_error(ctx, DISORDER_OOM, "decode: workspace too small");
+    if ((!cp.sum && !A) || !U) return dis_set_error(ctx, DISORDER_OOM, "decode: workspace too small");
     CoilArgs ca = coil_args(plan, sp.Sf, sp.C, 0, N3, V, n, d_seg);
-    DIS_TRY(dis_coil_scatter_ifft2(ctx, plan, ca, sp.y, plan->n_samples, 0, N3, sp.We, sp.Mb, A));
     const float scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
-    DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
+    if (cp.sum) {
+      DIS_TRY(dis_coil_sum_adj(ctx, plan, ca, sp.y, plan->n_samples, 0, N3, sp.We, sp.Mb, U, scale));
+    } else {
+      DIS_TRY(dis_coil_scatter_ifft2(ctx, plan, ca, sp.y, plan->n_samples, 0, N3, sp.We, sp.Mb, A));
+      DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
+    }
     int nm = 0;
     if (motion)
       for (int s : segs)
@@ -365,10 +413,13 @@ int dis_backproject_states(disorder_ctx_s* ctx, const disorder_plan_s* plan, con
   const int S = plan->n_mot;
   const int N3 = plan->N[2];
   if (S == 0) return DISORDER_OK;
-  const int ch = dis_chunk_slots(plan, C, N3, 0, S);
+  std::vector<int> all(S);
+  for (int j = 0; j < S; ++j) all[j] = j;
+  const CoilPlan cp = coil_plan(plan, C, N3, all);
+  const size_t coil = cp.sum ? 0 : cp.per_slot;
+  const int ch = cp.sum ? S : dis_chunk_slots(plan, C, N3, 0, S);
   Workspace ws;
-  DIS_TRY(dis_workspace(ctx, (size_t)ch * coil_slot_bytes(plan, C, N3) + dis_table_bytes(plan, ch, false) + 4096 * 4,
-                        &ws));
+  DIS_TRY(dis_workspace(ctx, (size_t)ch * coil + dis_table_bytes(plan, ch, false) + 4096 * 4, &ws));
   const float scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
   for (int c0 = 0; c0 < S; c0 += ch) {
     const int n = std::min(ch, S - c0);
@@ -377,12 +428,16 @@ int dis_backproject_states(disorder_ctx_s* ctx, const disorder_plan_s* plan, con
     for (int j = 0; j < n; ++j) st[j] = c0 + j;
     int* d_seg = nullptr;
     DIS_TRY(dis_upload_ints(ctx, &w, st, &d_seg));
-    float2* A = w.take<float2>((size_t)n * C * V);
-    if (!A) return dis_set_error(ctx, DISORDER_OOM, "back-projection: workspace too small");
     float2* U = out + (long long)c0 * V;
     CoilArgs ca = coil_args(plan, Sf, C, 0, N3, V, n, d_seg);
-    DIS_TRY(dis_coil_scatter_ifft2(ctx, plan, ca, r, plan->n_samples, 0, N3, nullptr, nullptr, A));
-    DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
+    if (cp.sum) {
+      DIS_TRY(dis_coil_sum_adj(ctx, plan, ca, r, plan->n_samples, 0, N3, nullptr, nullptr, U, scale));
+    } else {
+      float2* A = w.take<float2>((size_t)n * C * V);
+      if (!A) return dis_set_error(ctx, DISORDER_OOM, "back-projection: workspace too small");
+      DIS_TRY(dis_coil_scatter_ifft2(ctx, plan, ca, r, plan->n_samples, 0, N3, nullptr, nullptr, A));
+      DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
+    }
     if (dis_any_motion(T, S)) {
       std::vector<SlotParams> prm;
       dis_slot_params(T, S, st.data(), n, 0, &prm);
@@ -445,18 +500,28 @@ int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, 
     }
     return DISORDER_OK;
   }
-  const int ch = dis_chunk_slots(plan, sp.C, N3, V * sizeof(float2), nsg);
-  const size_t need = (size_t)ch * (coil_slot_bytes(plan, sp.C, N3) + V * sizeof(float2)) +
-                      2 * dis_table_bytes(plan, ch, false) + 4096 * 4;
+  const CoilPlan cp = coil_plan(plan, sp.C, N3, sp.segs);
+  const int ch = chunk_for(plan, cp.per_slot, V * sizeof(float2), nsg);
+  // the sample-sum stage goes through the samples E x: the caller's ys, or a
+  // buffer of all samples (each chunk writes and reads its own segments' rows)
+  const long long ny = plan->n_samples * N3 * (long long)sp.C;
+  const size_t ybuf = (cp.sum && !sp.ys) ? ((size_t)ny * sizeof(float2) + 256) : 0;
+  const size_t need = (size_t)ch * (cp.per_slot + V * sizeof(float2)) + 2 * dis_table_bytes(plan, ch, false) +
+                      ybuf + 4096 * 4;
   Workspace ws;
   DIS_TRY(dis_workspace(ctx, need, &ws));
+  float2* ysb = sp.ys;
+  if (cp.sum && !ysb) {
+    ysb = ws.take<float2>((size_t)ny);
+    if (!ysb) return dis_set_error(ctx, DISORDER_OOM, "encodedecode: workspace too small");
+  }
   for (int c0 = 0; c0 < nsg; c0 += ch) {
     const int n = std::min(ch, nsg - c0);
     Workspace w = ws;
     std::vector<int> segs(sp.segs.begin() + c0, sp.segs.begin() + c0 + n);
     int* d_seg = nullptr;
     DIS_TRY(dis_upload_ints(ctx, &w, segs, &d_seg));
-    float2* A = w.take<float2>((size_t)n * sp.C * V);
+    float2* A = w.take<float2>((size_t)n * cp.per_slot / sizeof(float2));
     if (!A) return dis_set_error(ctx, DISORDER_OOM, "encodedecode: workspace too small");
     const float2* z;
     long long Vz;
@@ -469,11 +534,19 @@ int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, 
       if (!U) return dis_set_error(ctx, DISORDER_OOM, "encodedecode: workspace too small");
     }
     CoilArgs ca = coil_args(plan, sp.Sf, sp.C, 0, N3, Vz, n, d_seg);
-    DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, z, A));
-    DIS_TRY(dis_coil_fft2_weight(ctx, plan, ca, A, sp.wmap, sp.ys, plan->n_samples, 0, N3));
-    ca.Vz = V;
-    const float scale = (float)(1.0 / ((double)plan->N[0] * plan->N[1]));
-    DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
+    if (cp.sum) {
+      // E x into the samples, then E^H W of them (encodedecode.m:125,133 apply EH.We)
+      const float s1 = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
+      DIS_TRY(dis_coil_sum_fwd(ctx, plan, ca, z, A, cp.ldp, ysb, plan->n_samples, 0, N3, nullptr, s1));
+      ca.Vz = V;
+      DIS_TRY(dis_coil_sum_adj(ctx, plan, ca, ysb, plan->n_samples, 0, N3, sp.We, nullptr, U, s1));
+    } else {
+      DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, z, A));
+      DIS_TRY(dis_coil_fft2_weight(ctx, plan, ca, A, sp.wmap, sp.ys, plan->n_samples, 0, N3));
+      ca.Vz = V;
+      const float scale = (float)(1.0 / ((double)plan->N[0] * plan->N[1]));
+      DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
+    }
     DIS_TRY(sum_back(ctx, plan, U, sp.T, sp.T_n, segs, nm, &w, out, &first));
   }
   return DISORDER_OK;

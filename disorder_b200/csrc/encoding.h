@@ -64,5 +64,13 @@ int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, 
 int dis_gradient(disorder_ctx_s* ctx, const disorder_plan_s* plan, const float2* x, long long x_s,
                  const Tables& tb, float2* z, float2* yB, float2* w1, float2* w2, float2* G);
 bool dis_plane_usable(const disorder_plan_s* plan, int C, const std::vector<int>& segs);
+// the sample-sum coil stage (sumcoil.cu): no per-coil intermediate volumes
+bool dis_sum_coil_usable(const disorder_plan_s* plan);
+size_t dis_sum_part_bytes(const disorder_plan_s* plan, int C, int N3c, int ldp);
+int dis_coil_sum_fwd(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* z,
+                     float2* part, int ldp, float2* y, long long y_ld, int y_n3off, int y_N3, const float2* y_meas,
+                     float scale);
+int dis_coil_sum_adj(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* y,
+                     long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* u, float scale);
 int dis_sum_slots(disorder_ctx_s* ctx, const float2* u, long long V, int n_slots, float2* out, float beta);
 int dis_broadcast(disorder_ctx_s* ctx, const float2* x, long long V, int n_slots, float2* out);

@@ -31,6 +31,8 @@ struct disorder_ctx_s {
   void* static_scratch = nullptr;
   size_t static_scratch_bytes = 0;
   int fault = 0;  // one-shot injected fault (disorder_ctx_inject_fault)
+  int precision = DISORDER_PRECISION_FP32;  // tensor-core contractions (disorder_ctx_set_precision)
+  int tune_tma = 1;  // strided line passes on TMA tiles (1) or cp.async pipelines (0) (disorder_ctx_set_tuning)
 };
 
 // Workspace bump allocator on top of the context's cached buffer.
@@ -215,6 +217,10 @@ int dis_seg_sums(disorder_ctx_s* ctx, const disorder_plan_s* plan, const int* d_
                  const float2* r, const float2* G /*nullable*/, long long G_stride, long long ld, int n3off, int N3c,
                  int N3full, int C, const float* wrow, double* d_out /*[n_slots][28]*/, Workspace* ws);
 
+
+// tensor-core Gram of compressCoils (umma_gram.cu): partials part[b][c*C+d]
+int dis_gram_umma(disorder_ctx_s* ctx, const float2* S, int C, long long V, float reg, double* part, int grid,
+                  int mode);
 
 // launch accounting
 inline void dis_count(disorder_ctx_s* ctx, int n = 1) { ctx->launches += n; }

@@ -362,13 +362,29 @@ int disorder_compress_coils(disorder_ctx ctx, const void* S, int32_t C_in, int64
   float2* dA = ws.take<float2>((size_t)np);
   if (!part || !dA) return dis_set_error(ctx, DISORDER_OOM, "compress_coils workspace");
   if (np > 8 * kThreads) return dis_set_error(ctx, DISORDER_BAD_ARG, "compress_coils: too many coils");
-  gram_kernel<<<nb, kThreads, 2 * kV * C_in * sizeof(float2), ctx->stream>>>((const float2*)S, C_in, V, 1e-9f, part);
-  dis_count(ctx);
-  std::vector<double> h((size_t)nb * np * 2);
+  int nb_used = nb;
+  if (ctx->precision != DISORDER_PRECISION_FP32) {
+    // the contraction on the tensor cores, one CTA per SM
+    nb_used = std::min(nb, ctx->sm_count);
+    DIS_TRY(dis_gram_umma(ctx, (const float2*)S, C_in, V, 1e-9f, part, nb_used, ctx->precision));
+  } else {
+    gram_kernel<<<nb, kThreads, 2 * kV * C_in * sizeof(float2), ctx->stream>>>((const float2*)S, C_in, V, 1e-9f,
+                                                                              part);
+    dis_count(ctx);
+  }
+  std::vector<double> h((size_t)nb_used * np * 2);
   DIS_CUDA_TRY(cudaMemcpyAsync(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (ctx->precision != DISORDER_PRECISION_FP32) {
+    int late = 0;
+    DIS_CUDA_TRY(cudaMemcpy(&late, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (late) {
+      DIS_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(int)));
+      return dis_set_error(ctx, DISORDER_TIMEOUT, "compress_coils: a tensor-core MMA wait ran out");
+    }
+  }
   std::vector<std::complex<double>> P((size_t)np, 0.0);
-  for (int b = 0; b < nb; ++b)
+  for (int b = 0; b < nb_used; ++b)
     for (int p = 0; p < np; ++p) P[p] += std::complex<double>(h[((size_t)b * np + p) * 2], h[((size_t)b * np + p) * 2 + 1]);
   // P(c,d) with p = c*C + d -> column-major matrix M(c,d)
   std::vector<std::complex<double>> M((size_t)np);

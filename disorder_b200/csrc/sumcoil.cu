@@ -1,0 +1,335 @@
+// Coil stage of the encoding operators without per-coil intermediate volumes.
+//
+// encode (Reconstruction/encode.m:90-136) evaluates, per motion state s, coil
+// c and readout position n3, the unitary 2-D DFT of S_c .* z_s at the state's
+// samples (ky_i, kz_i) only:
+//   y_i = (N1 N2)^(-1/2) sum_b W2^{kz_i b} X[ky_i, b],  X = FFT_1(S_c .* z_s),
+// and decode (decode.m:42-58,78-85) is its adjoint. The three-pass coil stage
+// writes X for every coil (8 V C bytes per state) and reads it back three
+// times. Here the dim-2 sum is split over tiles of LPB adjacent b (the lines
+// of one CTA, along dim 1):
+//   forward: a CTA loads its LPB lines of z_s once, and per coil multiplies by
+//     S_c, FFTs along dim 1 in registers, puts X[b, ky] in shared memory and
+//     adds sum_{b in tile} W2^{kz_i b} X[b, ky_i] for every sample i of the
+//     state (threads walk the samples in ky order, so a warp reads a few
+//     neighbouring rows of X); the tile's partial sums go to a buffer
+//     part[slot][tile][c][n3][q] (q: the sample's place in ky order), and a
+//     reduction adds the N2 / LPB tiles into y (times the DFT scale, minus the
+//     measured samples when given);
+//   adjoint: per coil the CTA rebuilds its LPB columns of X from the samples,
+//     one thread per ky row (each row's samples are contiguous in ky order,
+//     so no two threads write the same element), X[b, ky] = sum_{i in row ky}
+//     w_i y_i conj(W2^{kz_i b}), inverse-FFTs along dim 1 and accumulates
+//     conj(S_c) .* (...) over the coils in registers; one store of u.
+// Per state this moves 8 V (z) + 8 V (u) + the coil maps (shared by the
+// states of a tile through L2) + the partial sums (N2 / LPB x the samples),
+// against 40 V C for the three passes.
+#include <cmath>
+
+#include "encoding.h"
+#include "fastpass.cuh"
+#include "fastpass.h"
+#include "internal.h"
+
+namespace sc {
+
+using fp::kThreads;
+
+struct SumArgs {
+  int N1, N2, N3c;
+  long long Vz;          // slot stride of z / u
+  const float2* Sf;      // coil maps, offset to the chunk's first readout row
+  long long Sc;          // coil stride of Sf
+  int C;
+  int n_slots;
+  const int* slot_seg;   // segment of each slot
+  const int* rowptr;     // per-segment CSR over ky rows (global sample positions)
+  const int* perm;       // sample index at each CSR position
+  const int* ky;
+  const int* kz;
+  const float2* tw2;     // W_N2^m, m < N2
+  float2* part;          // [slot][tile][c][n3][q]
+  int ldp;               // q stride (most samples of a chunk segment)
+  int ntile;             // N2 / LPB
+};
+
+// forward: partial sample sums of one (slot, tile of LPB lines along b, n3)
+template <int F1, int F2>
+__global__ void __launch_bounds__(kThreads) sum_fwd_kernel(SumArgs a, const float2* __restrict__ z,
+                                                           const float2* __restrict__ twg) {
+  using LN = ff::Line<F1, F2>;
+  constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
+  extern __shared__ __align__(16) float2 sm[];
+  float2* tw = sm;
+  float2* ex = tw + LN::TWS;
+  float2* Xs = ex + LPB * LN::EXSZ;  // [LPB][N]: X[b0 + j, ky]
+  const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
+  ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
+  const int slot = (int)(blockIdx.x % a.n_slots);
+  const long long q0 = (long long)(blockIdx.x / a.n_slots) * LPB;  // first line (b + N2 n3)
+  const int n3 = (int)(q0 / a.N2), b0 = (int)(q0 % a.N2), tile = b0 / LPB;
+  const long long base = (q0 + li) * N;
+  float2* myex = ex + li * LN::EXSZ;
+  const int seg = a.slot_seg[slot];
+  const int* rp = a.rowptr + (long long)seg * (a.N1 + 1);
+  const int s0 = rp[0], s1 = rp[a.N1];
+  __syncthreads();
+  const float2* zs = z + slot * a.Vz;
+  float2 zr[F1];
+#pragma unroll
+  for (int m = 0; m < F1; ++m) zr[m] = lt < F2 ? zs[base + lt + F2 * m] : make_float2(0.f, 0.f);
+  for (int c = 0; c < a.C; ++c) {
+    const float2* S = a.Sf + c * a.Sc;
+    float2 v[F1], X[F2];
+#pragma unroll
+    for (int m = 0; m < F1; ++m) v[m] = lt < F2 ? cmul(S[base + lt + F2 * m], zr[m]) : make_float2(0.f, 0.f);
+    LN::fwd(v, X, lt, myex, tw);
+    if (lt < F1) {
+#pragma unroll
+      for (int k2 = 0; k2 < F2; ++k2) Xs[li * N + lt + F1 * k2] = X[k2];
+    }
+    __syncthreads();
+    float2* out = a.part + ((((long long)slot * a.ntile + tile) * a.C + c) * a.N3c + n3) * a.ldp;
+    for (int q = s0 + tid; q < s1; q += kThreads) {
+      const int i = a.perm[q];
+      const int ky = a.ky[i], kz = a.kz[i];
+      int e = (int)(((long long)kz * b0) % a.N2);
+      float2 w = a.tw2[e];
+      const float2 st = a.tw2[kz];
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < LPB; ++j) {
+        acc = cfma(w, Xs[j * N + ky], acc);
+        w = cmul(w, st);
+      }
+      out[q - s0] = acc;
+    }
+    __syncthreads();  // Xs and the exchange area are rewritten by the next coil
+  }
+}
+
+// y[i + ld (n3 + n3off + N3y c)] = scale * sum over tiles of part (- ymeas)
+__global__ void sum_reduce_kernel(SumArgs a, float2* __restrict__ y, const float2* __restrict__ ymeas, long long ld,
+                                  int n3off, int N3y, float scale) {
+  const long long per_slot = (long long)a.C * a.N3c * a.ldp;
+  const long long tot = per_slot * a.n_slots;
+  const long long ts = (long long)a.C * a.N3c * a.ldp;  // tile stride
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+    const int slot = (int)(e / per_slot);
+    const long long r = e % per_slot;  // (c, n3, q)
+    const int q = (int)(r % a.ldp);
+    const long long cn = r / a.ldp;
+    const int n3 = (int)(cn % a.N3c), c = (int)(cn / a.N3c);
+    const int seg = a.slot_seg[slot];
+    const int* rp = a.rowptr + (long long)seg * (a.N1 + 1);
+    if (q >= rp[a.N1] - rp[0]) continue;
+    const float2* p = a.part + (long long)slot * a.ntile * ts + r;
+    float2 s = make_float2(0.f, 0.f);
+    for (int t = 0; t < a.ntile; ++t) s = cadd(s, p[t * ts]);
+    const int i = a.perm[rp[0] + q];
+    const long long o = i + ld * (n3 + n3off) + ld * N3y * c;
+    float2 v = cscale(s, scale);
+    if (ymeas) v = csub(v, ymeas[o]);
+    y[o] = v;
+  }
+}
+
+// adjoint: u[slot] (LPB lines) = scale * sum_c conj(S_c) .* IFFT_1(X_c), X_c
+// built from the weighted samples of the slot's segment
+template <int F1, int F2>
+__global__ void __launch_bounds__(kThreads) sum_adj_kernel(SumArgs a, const float2* __restrict__ y, long long ld,
+                                                           int n3off, int N3y, const float* __restrict__ We,
+                                                           const float* __restrict__ Mb, float2* __restrict__ u,
+                                                           float scale, const float2* __restrict__ twg) {
+  using LN = ff::Line<F1, F2>;
+  constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
+  extern __shared__ __align__(16) float2 sm[];
+  float2* tw = sm;
+  float2* ex = tw + LN::TWS;
+  float2* Xs = ex + LPB * LN::EXSZ;  // [LPB][N]
+  const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
+  ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
+  const int slot = (int)(blockIdx.x % a.n_slots);
+  const long long q0 = (long long)(blockIdx.x / a.n_slots) * LPB;
+  const int n3 = (int)(q0 / a.N2), b0 = (int)(q0 % a.N2);
+  const long long base = (q0 + li) * N;
+  float2* myex = ex + li * LN::EXSZ;
+  const int seg = a.slot_seg[slot];
+  const int* rp = a.rowptr + (long long)seg * (a.N1 + 1);
+  const float mb = Mb ? Mb[n3 + n3off] : 1.f;
+  __syncthreads();
+  float2 acc[F1];
+#pragma unroll
+  for (int m = 0; m < F1; ++m) acc[m] = make_float2(0.f, 0.f);
+  for (int c = 0; c < a.C; ++c) {
+    const long long yo = ld * (n3 + n3off) + ld * N3y * c;
+    for (int r = tid; r < a.N1; r += kThreads) {
+      float2 xr[LPB];
+#pragma unroll
+      for (int j = 0; j < LPB; ++j) xr[j] = make_float2(0.f, 0.f);
+      for (int q = rp[r]; q < rp[r + 1]; ++q) {
+        const int i = a.perm[q];
+        const int kz = a.kz[i];
+        const float2 val = cscale(y[yo + i], We ? mb * We[i] : mb);
+        int e = (int)(((long long)kz * b0) % a.N2);
+        float2 w = cconj(a.tw2[e]);
+        const float2 st = cconj(a.tw2[kz]);
+        float2 vw = cmul(val, w);
+#pragma unroll
+        for (int j = 0; j < LPB; ++j) {
+          xr[j] = cadd(xr[j], vw);
+          vw = cmul(vw, st);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < LPB; ++j) Xs[j * N + r] = xr[j];
+    }
+    __syncthreads();
+    float2 X[F2], v[F1];
+#pragma unroll
+    for (int k2 = 0; k2 < F2; ++k2) X[k2] = lt < F1 ? Xs[li * N + lt + F1 * k2] : make_float2(0.f, 0.f);
+    __syncthreads();  // the next coil rewrites Xs
+    LN::inv(X, v, lt, myex, tw);
+    if (lt < F2) {
+      const float2* S = a.Sf + c * a.Sc + base;
+#pragma unroll
+      for (int m = 0; m < F1; ++m) acc[m] = cadd(acc[m], cmulc(v[m], S[lt + F2 * m]));
+    }
+  }
+  if (lt < F2) {
+    float2* o = u + slot * a.Vz + base;
+#pragma unroll
+    for (int m = 0; m < F1; ++m) o[lt + F2 * m] = cscale(acc[m], scale);
+  }
+}
+
+template <int F1, int F2>
+struct SumLaunch {
+  using LN = ff::Line<F1, F2>;
+  static constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
+  static size_t smem() { return sizeof(float2) * (LN::TWS + (size_t)LPB * LN::EXSZ + (size_t)LPB * N); }
+  static bool init() {
+    const int b = (int)smem();
+    return cudaFuncSetAttribute(sum_fwd_kernel<F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(sum_adj_kernel<F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) == cudaSuccess;
+  }
+  static bool fwd(const SumArgs& a, const float2* z, const float2* tw, cudaStream_t s) {
+    static const bool ok = init();
+    if (!ok) return false;
+    const unsigned grid = (unsigned)(((long long)a.N2 * a.N3c / LPB) * a.n_slots);
+    sum_fwd_kernel<F1, F2><<<grid, kThreads, smem(), s>>>(a, z, tw);
+    return true;
+  }
+  static bool adj(const SumArgs& a, const float2* y, long long ld, int n3off, int N3y, const float* We,
+                  const float* Mb, float2* u, float scale, const float2* tw, cudaStream_t s) {
+    static const bool ok = init();
+    if (!ok) return false;
+    const unsigned grid = (unsigned)(((long long)a.N2 * a.N3c / LPB) * a.n_slots);
+    sum_adj_kernel<F1, F2><<<grid, kThreads, smem(), s>>>(a, y, ld, n3off, N3y, We, Mb, u, scale, tw);
+    return true;
+  }
+};
+
+// lines per CTA for a dim-1 length, 0 when no kernel exists
+int lines_per_cta(int n1) {
+  int F1, F2;
+  if (!dis_fast_factor(n1, &F1, &F2)) return 0;
+  return kThreads / ff::pow2ceil(F1 > F2 ? F1 : F2);
+}
+
+template <class Fn>
+bool dispatch(int n1, Fn&& f) {
+  switch (n1) {
+    case 16: return f(SumLaunch<4, 4>());
+    case 32: return f(SumLaunch<8, 4>());
+    case 44: return f(SumLaunch<4, 11>());
+    case 64: return f(SumLaunch<8, 8>());
+    case 88: return f(SumLaunch<8, 11>());
+    case 96: return f(SumLaunch<8, 12>());
+    case 128: return f(SumLaunch<16, 8>());
+    case 160: return f(SumLaunch<16, 10>());
+    case 176: return f(SumLaunch<16, 11>());
+    case 192: return f(SumLaunch<16, 12>());
+    case 256: return f(SumLaunch<16, 16>());
+    default: return false;
+  }
+}
+
+}  // namespace sc
+
+// The sample-sum coil stage needs a dim-1 line kernel, N2 a multiple of the
+// lines per CTA, one thread per ky row at most 4 rows a thread, and the
+// partial buffer's tile count; DISORDER_THREE_PASS=1 keeps the three-pass
+// stage (the comparison path of the tests).
+bool dis_sum_coil_usable(const disorder_plan_s* plan) {
+  static int off = -1;
+  if (off < 0) {
+    const char* e = std::getenv("DISORDER_THREE_PASS");
+    off = (e && e[0] == '1') ? 1 : 0;
+  }
+  if (off || !dis_use_fast()) return false;
+  const int lpb = sc::lines_per_cta(plan->N[0]);
+  return lpb > 0 && plan->N[1] % lpb == 0 && plan->N[0] <= 4 * fp::kThreads;
+}
+
+// bytes of partial sums per slot for C coils, N3c readout rows and ldp samples
+size_t dis_sum_part_bytes(const disorder_plan_s* plan, int C, int N3c, int ldp) {
+  const int lpb = sc::lines_per_cta(plan->N[0]);
+  return (size_t)(plan->N[1] / std::max(lpb, 1)) * C * N3c * (size_t)ldp * sizeof(float2);
+}
+
+static sc::SumArgs sum_args(const disorder_plan_s* plan, const CoilArgs& a, float2* part, int ldp) {
+  sc::SumArgs s;
+  s.N1 = a.N1;
+  s.N2 = a.N2;
+  s.N3c = a.N3c;
+  s.Vz = a.Vz;
+  s.Sf = a.Sf;
+  s.Sc = a.Sc;
+  s.C = a.C;
+  s.n_slots = a.n_slots;
+  s.slot_seg = a.d_slot_seg;
+  s.rowptr = plan->d_rowptr;
+  s.perm = plan->d_perm;
+  s.ky = plan->d_ky;
+  s.kz = plan->d_kz;
+  s.tw2 = plan->d_tw[1];
+  s.part = part;
+  s.ldp = ldp;
+  s.ntile = a.N2 / std::max(sc::lines_per_cta(a.N1), 1);
+  return s;
+}
+
+// encode's coil stage: y (the chunk's slots' samples, rows n3off.. of y) from
+// the state volumes z (first readout row of the chunk)
+int dis_coil_sum_fwd(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* z,
+                     float2* part, int ldp, float2* y, long long y_ld, int y_n3off, int y_N3, const float2* y_meas,
+                     float scale) {
+  if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
+  const sc::SumArgs s = sum_args(plan, a, part, ldp);
+  const bool ok = sc::dispatch(a.N1, [&](auto L) { return decltype(L)::fwd(s, z, plan->d_tw[0], ctx->stream); });
+  if (!ok) return dis_set_error(ctx, DISORDER_BAD_ARG, "sample-sum coil stage: no kernel for N1=%d", a.N1);
+  dis_count(ctx);
+  const long long tot = (long long)a.n_slots * a.C * a.N3c * ldp;
+  const int blocks = (int)std::min<long long>((tot + 255) / 256, 8LL * ctx->sm_count);
+  sc::sum_reduce_kernel<<<std::max(blocks, 1), 256, 0, ctx->stream>>>(s, y, y_meas, y_ld, y_n3off, y_N3, scale);
+  dis_count(ctx);
+  DIS_CUDA_TRY(cudaGetLastError());
+  return DISORDER_OK;
+}
+
+// decode's coil stage: u (slot volumes, first readout row of the chunk) from
+// the samples y weighted by We (per sample) and Mb (per readout row)
+int dis_coil_sum_adj(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* y,
+                     long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* u, float scale) {
+  if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
+  const sc::SumArgs s = sum_args(plan, a, nullptr, 0);
+  const bool ok = sc::dispatch(a.N1, [&](auto L) {
+    return decltype(L)::adj(s, y, y_ld, y_n3off, y_N3, We, Mb, u, scale, plan->d_tw[0], ctx->stream);
+  });
+  if (!ok) return dis_set_error(ctx, DISORDER_BAD_ARG, "sample-sum coil stage: no kernel for N1=%d", a.N1);
+  dis_count(ctx);
+  DIS_CUDA_TRY(cudaGetLastError());
+  return DISORDER_OK;
+}

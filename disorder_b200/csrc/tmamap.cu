@@ -92,8 +92,11 @@ static void take_fault(disorder_ctx_s* ctx, fp::TArgs& t) {
   }
 }
 
+bool dis_umma_line(int n, int mode, const CUtensorMap& in, const CUtensorMap& out, const fp::TArgs& t,
+                   const float2* tw, int shared_input, int sm_count, cudaStream_t s);
+
 bool dis_fast_tma_line(disorder_ctx_s* ctx, const LinePassArgs& a) {
-  if (!tma_enabled() || !ctx->d_err) return false;
+  if (!tma_enabled() || !ctx->tune_tma || !ctx->d_err) return false;
   if (a.axis == 0 || a.accumulate || a.in1 || a.out1 || a.c01 != P_ZERO) return false;
   if (!a.Sd.p || !(a.c00 == P_A || a.c00 == P_ONE)) return false;
   const int n = a.N[a.axis];
@@ -115,12 +118,16 @@ bool dis_fast_tma_line(disorder_ctx_s* ctx, const LinePassArgs& a) {
   t.a = a;
   t.err = ctx->d_err;
   take_fault(ctx, t);
+  // mixed precision: the DFTs of the pass as tensor-core GEMMs where a kernel exists
+  if (ctx->precision != DISORDER_PRECISION_FP32 && F1 == 16 &&
+      dis_umma_line(n, ctx->precision, in, out, t, a.tw, shared_input, ctx->sm_count, ctx->stream))
+    return true;
   return launch_size(n, 0, in, out, t, a.tw, shared_input, ctx->stream);
 }
 
 bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, const float* wmap, const float2* tw,
                          const disorder_plan_s* plan, float2* ys, long long ld, int n3off, int N3y, float scale) {
-  if (!tma_enabled() || !ctx->d_err || !has_tma_size(a.N2)) return false;
+  if (!tma_enabled() || !ctx->tune_tma || !ctx->d_err || !has_tma_size(a.N2)) return false;
   const int Nv[3] = {a.N1, a.N2, a.N3c};
   const long long Vc = (long long)a.N1 * a.N2 * a.N3c;
   const long long nvol = (long long)a.n_slots * a.C;
@@ -154,7 +161,7 @@ bool dis_fast_tma_weight(disorder_ctx_s* ctx, const CoilArgs& a, float2* A, cons
 namespace {
 bool coil_tma(disorder_ctx_s* ctx, int kind, const CoilArgs& a, float2* A, const disorder_plan_s* plan,
               fp::TArgs& t) {
-  if (!tma_enabled() || !ctx->d_err || !has_tma_size(a.N2)) return false;
+  if (!tma_enabled() || !ctx->tune_tma || !ctx->d_err || !has_tma_size(a.N2)) return false;
   const int Nv[3] = {a.N1, a.N2, a.N3c};
   const long long Vc = (long long)a.N1 * a.N2 * a.N3c;
   const long long nvol = (long long)a.n_slots * a.C;

@@ -92,20 +92,30 @@ def tile_shape(n_shots):
     return b1, n_shots // b1
 
 
-def random_checkered(NY, n_shots, rng):
+def random_checkered(NY, n_shots, rng, truncate=False):
     """Simulation/synthesizeEncoding.m:86-106,127: returns the (NY1, NY2)
-    array of 1-based shot indices with DC first (ifftshifted)."""
+    array of 1-based shot indices with DC first (ifftshifted).
+
+    The reference requires tiles that divide the grid. With truncate=True a
+    grid that the b1 x b2 tile does not divide is covered by
+    ceil(NY1/b1) x ceil(NY2/b2) tiles whose last row and column are cut at the
+    grid edge: every full tile still gives each shot one position, and an edge
+    tile gives its positions to the shots of its permutation that land
+    inside the grid (the rectangular variant used for shot counts such as 96
+    on a 128 x 160 grid)."""
     b1, b2 = tile_shape(n_shots)
     NY1, NY2 = int(NY[0]), int(NY[1])
-    if NY1 % b1 or NY2 % b2:
+    if (NY1 % b1 or NY2 % b2) and not truncate:
         raise ValueError("grid %dx%d is not tiled by %dx%d" % (NY1, NY2, b1, b2))
     H = np.zeros((NY1, NY2), np.int32)
-    for o in range(NY1 // b1):
-        for p in range(NY2 // b2):
+    for o in range(-(-NY1 // b1)):
+        for p in range(-(-NY2 // b2)):
             perm = rng.permutation(n_shots)  # indRand = randperm(NNT)
             IR, JR = np.unravel_index(perm, (b1, b2), order="F")  # ind2sub
             s = np.arange(n_shots)
-            H[IR + o * b1, JR + p * b2] = s + 1
+            r, c = IR + o * b1, JR + p * b2
+            keep = (r < NY1) & (c < NY2)
+            H[r[keep], c[keep]] = s[keep] + 1
     return np.fft.ifftshift(H)
 
 

@@ -1,60 +1,87 @@
-"""Fast synthesis of large scans on the GPU with torch (same recipe as
-disorder_b200.synth, used by the benchmark to build 256x256x176 inputs in
-seconds). Only the phantom and coil maps are built here; sampling, motion and
-noise levels come from disorder_b200.synth."""
+"""Synthetic scans built on the GPU by the library's own kernels
+(disorder_synth_phantom, disorder_synth_coils, disorder_add_noise).
+
+The random parameters are drawn on the host with the same generator calls, in
+the same order, as the NumPy recipe in disorder_b200.synth (phantom: per
+ellipsoid centre, semi-axes, rotation angles and magnitude, then four phase
+terms; coils: per coil a wave vector and a phase), so a scan built here from
+numpy.random.default_rng(seed) matches synth.phantom / synth.coil_maps from
+the same seed up to single-precision rounding. Sampling and motion come from
+disorder_b200.synth (host, cheap); the noise is drawn on the device.
+"""
+
+import ctypes as C
+import math
 
 import numpy as np
 
-
-def _grid(N, dev):
-    import torch
-    ax = [torch.linspace(-0.5, 0.5, n + 1, device=dev, dtype=torch.float32)[:-1] for n in N]
-    return torch.meshgrid(*ax, indexing="ij")
+from . import _lib
+from .synth import _rot
 
 
-def phantom_torch(N, n_ellipsoids, rng, dev="cuda"):
-    import torch
-    from .synth import _rot
-    X, Y, Z = _grid(N, dev)
-    mag = torch.zeros(N, device=dev)
-    for _ in range(n_ellipsoids):
+def phantom_params(n_ellipsoids, rng):
+    """(ellipsoids (n, 16) float32, phase terms (4, 5) float32) drawn as
+    synth.phantom draws them."""
+    ell = np.zeros((n_ellipsoids, 16), np.float32)
+    for q in range(n_ellipsoids):
         c = rng.uniform(-0.2, 0.2, 3)
         ax = rng.uniform(0.04, 0.25, 3)
-        R = _rot(*rng.uniform(-np.pi, np.pi, 3))
-        dx, dy, dz = X - c[0], Y - c[1], Z - c[2]
-        u = (R[0, 0] * dx + R[0, 1] * dy + R[0, 2] * dz) / ax[0]
-        v = (R[1, 0] * dx + R[1, 1] * dy + R[1, 2] * dz) / ax[1]
-        w = (R[2, 0] * dx + R[2, 1] * dy + R[2, 2] * dz) / ax[2]
-        mag += float(rng.uniform(0.2, 1.0)) * ((u * u + v * v + w * w) <= 1.0).float()
-    ph = torch.zeros(N, device=dev)
-    for _ in range(4):
-        f = rng.uniform(0.3, 1.5, 3)
-        p0 = rng.uniform(-np.pi, np.pi)
-        a = rng.uniform(0.2, 0.6)
-        ph += float(a) * torch.cos(2 * np.pi * (f[0] * X + f[1] * Y + f[2] * Z) + float(p0))
-    x = torch.polar(mag, ph)
-    return x / torch.linalg.vector_norm(x)
+        R = _rot(*rng.uniform(-np.pi, np.pi, 3)).astype(np.float32)
+        ell[q, 0:3] = c
+        ell[q, 3:6] = ax
+        ell[q, 6:15] = R.reshape(-1)
+        ell[q, 15] = np.float32(rng.uniform(0.2, 1.0))
+    ph = np.zeros((4, 5), np.float32)
+    for q in range(4):
+        ph[q, 0:3] = rng.uniform(0.3, 1.5, 3)
+        ph[q, 3] = rng.uniform(-np.pi, np.pi)
+        ph[q, 4] = rng.uniform(0.2, 0.6)
+    return ell, ph
 
 
-def coils_torch(N, n_coils, rng, width=0.45, dev="cuda"):
-    import torch
-    X, Y, Z = _grid(N, dev)
-    S = torch.zeros(tuple(N) + (n_coils,), device=dev, dtype=torch.complex64)
+def coil_params(n_coils, rng):
+    """(n_coils, 7) float32: centre on a sphere (Fibonacci directions, radius
+    0.6), wave vector and phase, as synth.coil_maps draws them."""
+    cp = np.zeros((n_coils, 7), np.float32)
     ga = np.pi * (3 - np.sqrt(5))
     for c in range(n_coils):
         zc = 1 - 2 * (c + 0.5) / n_coils
         rc = np.sqrt(max(0.0, 1 - zc * zc))
         th = ga * c
-        cen = 0.6 * np.array([rc * np.cos(th), rc * np.sin(th), zc])
-        d2 = (X - cen[0]) ** 2 + (Y - cen[1]) ** 2 + (Z - cen[2]) ** 2
-        g = torch.exp(-d2 / (2 * width ** 2))
-        k = rng.uniform(-2, 2, 3)
-        ph = 2 * np.pi * (k[0] * X + k[1] * Y + k[2] * Z) * 0.25 + float(rng.uniform(-np.pi, np.pi))
-        S[..., c] = torch.polar(g, ph)
-    rss = torch.sqrt(torch.sum(torch.abs(S) ** 2, dim=3, keepdim=True))
-    return S / rss
+        cp[c, 0:3] = 0.6 * np.array([rc * np.cos(th), rc * np.sin(th), zc])
+        cp[c, 3:6] = rng.uniform(-2, 2, 3)
+        cp[c, 6] = rng.uniform(-np.pi, np.pi)
+    return cp
 
 
-def to_fortran_numpy(t):
-    """torch tensor (MATLAB dim order) -> Fortran-ordered numpy array."""
-    return np.asfortranarray(t.detach().cpu().numpy())
+def phantom(ctx, N, n_ellipsoids, rng, normalise=True):
+    """The ellipsoid phantom as a device volume (N1, N2, N3), unit L2 norm
+    when normalise (fig0506.m:95)."""
+    ell, ph = phantom_params(n_ellipsoids, rng)
+    out = ctx.empty(tuple(N))
+    Nc = (C.c_int32 * 3)(*[int(n) for n in N])
+    ctx.check(ctx.lib.disorder_synth_phantom(ctx.h, Nc, int(n_ellipsoids), ell.ctypes.data_as(_lib.FP), 4,
+                                             ph.ctypes.data_as(_lib.FP), 1 if normalise else 0, out.ptr))
+    return out
+
+
+def coil_maps(ctx, N, n_coils, rng, width=0.45):
+    """Gaussian-bump coil maps (N1, N2, N3, C) with unit root sum of squares."""
+    cp = coil_params(n_coils, rng)
+    S = ctx.empty(tuple(N) + (int(n_coils),))
+    Nc = (C.c_int32 * 3)(*[int(n) for n in N])
+    ctx.check(ctx.lib.disorder_synth_coils(ctx.h, Nc, int(n_coils), cp.ctypes.data_as(_lib.FP), float(width), S.ptr))
+    return S
+
+
+def add_noise(ctx, y, sigma, seed):
+    """y += sigma * (n1 + i n2) in place (Methods/plugNoise.m:17)."""
+    ctx.check(ctx.lib.disorder_add_noise(ctx.h, y.ptr, int(np.prod(y.shape)), float(sigma), int(seed) & (2**64 - 1)))
+
+
+def snr_sigma(snr_db, V, ridge=1e-3):
+    """synth.snr_to_sigma for a unit-norm image of V voxels and coils with unit
+    root sum of squares: mean |x|^2 = 1/V and mean 1/(sum|S|^2 + 1e-3) =
+    1/(1 + 1e-3) (Simulation/SNRToLevels.m:23-33, unitary encoding)."""
+    meanN = (1.0 / V) / (10 ** (snr_db / 10))
+    return float(math.sqrt(meanN / (2.0 / (1.0 + ridge))))

@@ -84,6 +84,28 @@ typedef enum {
   DISORDER_FAULT_OOM = 2
 } disorder_fault;
 int disorder_ctx_inject_fault(disorder_ctx ctx, int32_t fault);
+/* Arithmetic of the contractions that can run on the tensor cores (no
+ * reference counterpart; the reference computes them in single precision):
+ * DISORDER_PRECISION_FP32 (default): FP32 on the CUDA cores.
+ * DISORDER_PRECISION_BF16X3: tcgen05 MMAs on operands split into two BF16
+ *   parts, hi*hi + hi*lo + lo*hi accumulated in FP32 (about 16 significant
+ *   bits per operand).
+ * DISORDER_PRECISION_TF32X3: the same with two TF32 parts (about 21 bits).
+ * The setting applies to the coil-compression Gram matrix
+ * (disorder_compress_coils) and to the DFT line passes of the sinc rigid
+ * transform that have a tensor-core kernel. */
+typedef enum {
+  DISORDER_PRECISION_FP32 = 0,
+  DISORDER_PRECISION_BF16X3 = 1,
+  DISORDER_PRECISION_TF32X3 = 2
+} disorder_precision;
+int disorder_ctx_set_precision(disorder_ctx ctx, int32_t mode);
+/* Kernel choices of one context, set by an autotuner (no reference
+ * counterpart). DISORDER_TUNE_TMA: 1 (default) moves the tiles of the strided
+ * line passes with TMA bulk tensor copies, 0 with per-thread cp.async
+ * pipelines (same results). */
+typedef enum { DISORDER_TUNE_TMA = 0 } disorder_tune_key;
+int disorder_ctx_set_tuning(disorder_ctx ctx, int32_t key, int32_t value);
 /* bytes of device workspace the context holds (operator, solver and reduction
  * buffers it grows on demand and keeps until disorder_ctx_destroy); a
  * diagnostic with no reference counterpart */
@@ -294,6 +316,28 @@ int disorder_residual_energies(disorder_ctx ctx, disorder_plan plan, const void*
 int disorder_backproject_states(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
                                 int32_t n_coils, const void* x, const float* T, int32_t n3_lo,
                                 int32_t n3_hi, void* out);
+
+/* ---- synthetic scan data (the simulation recipe on the device) ----
+ * The reference simulates acquisitions from a ground-truth image and coil
+ * maps it loads from files (fig0506.m:53-56) and adds complex Gaussian noise
+ * (Methods/plugNoise.m:17, Simulation/synthesizeY.m:82-84); these build the
+ * stand-ins on the device. N: host int32[3]; out/S/y: device.
+ * disorder_synth_phantom: out[v] = (sum over ellipsoids containing v of
+ *   their magnitude) * exp(i sum_q a_q cos(2 pi f_q . r + p0_q)), r the grid
+ *   coordinate -0.5 + i/N per axis. ell: host n_ell x 16 floats {centre[3],
+ *   semi-axes[3], rotation R (row-major 3x3), magnitude}, a point is inside
+ *   when |R (r - centre) / semi-axes| <= 1; ph: host n_ph x 5 floats {f[3],
+ *   p0, a}. normalise != 0 divides the volume by its L2 norm.
+ * disorder_synth_coils: S[v + c V] = g_c(v) exp(i phi_c(v)) / rss(v) with
+ *   g_c = exp(-|r - centre_c|^2 / (2 width^2)), phi_c = 2 pi k_c . r / 4 +
+ *   phase0_c, rss the root sum of squares of the g_c. cp: host C x 7 floats
+ *   {centre[3], k[3], phase0}.
+ * disorder_add_noise: y[e] += sigma (n1 + i n2), n1 and n2 standard normals
+ *   that depend only on (seed, e). */
+int disorder_synth_phantom(disorder_ctx ctx, const int32_t* N, int32_t n_ell, const float* ell, int32_t n_ph,
+                           const float* ph, int32_t normalise, void* out);
+int disorder_synth_coils(disorder_ctx ctx, const int32_t* N, int32_t C, const float* cp, float width, void* S);
+int disorder_add_noise(disorder_ctx ctx, void* y, int64_t n, float sigma, uint64_t seed);
 
 /* ---- learned motion proposal (no counterpart in the reference) ----
  * A 3-D convolutional network maps one state's back-projected residual and

@@ -93,11 +93,12 @@ def test_transform_at_benchmark_sizes(ctx, N, S):
     assert rel(back, backo) < TOL
 
 
-@pytest.mark.parametrize("N,C,shots,S", [((256, 256, 176), 16, 64, 2), ((128, 128, 88), 8, 64, 4)])
+@pytest.mark.parametrize("N,C,shots,S", [((256, 256, 176), 16, 64, 2), ((128, 128, 88), 8, 64, 4),
+                                         ((64, 64, 44), 16, 64, 8)])
 def test_operators_at_benchmark_sizes(ctx, N, C, shots, S):
     """encode, decode (with We and Mb) and encodedecode (with We) against the
-    oracle: the expand, weighted dim-2, gather, scatter and combine passes at
-    the benchmark's line lengths and coil counts."""
+    oracle: the coil stage (sample sums of the per-tile dim-2 DFT and their
+    adjoint) at the benchmark's line lengths and coil counts."""
     import disorder_b200 as db
     from oracle import encoding as oenc
     Ed, Eo, x = _problem(ctx, N, C, shots, S, seed=N[0] + C)
