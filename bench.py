@@ -304,6 +304,46 @@ def oracle_check(ctx, x, Eo, ed_oracle):
     return out
 
 
+def config1_run(ctx):
+    """The small simulation case end to end: 64^3, 12 ellipsoids, 8 coils, 16
+    random-checkered shots, rotations U(-3,3) deg, translations U(-3,3)
+    voxels, 30 dB, 10 outer iterations of CGsolver (3 iterations) + LMsolver
+    (1 iteration) at one resolution. The library's run (CUDA events) and the
+    FP64 oracle's run of the same schedule (wall time, all host threads) on
+    the same single-precision samples; relative difference of the final image
+    and motion, and the NRMSE of both."""
+    from disorder_b200 import recon, synth
+    from oracle import encoding as oenc
+    from oracle import grids as og
+    from oracle import solvers as osol
+    from oracle.encoding import Struct as OStruct
+    N, C, S = (64, 64, 64), 8, 16
+    sc = synth.make_scan(N, C, S, 3.0, 3.0, 30.0, 12, 1001)
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    Eo = OStruct(Tr=sc.T_gt, NMs=S, NSe=S + 1, Sf=sc.S.astype(np.complex128), ky=sc.ky, kz=sc.kz, nEc=sc.nEc,
+                 mSt=sc.mSt, grids=og.generateTransformGrids(N, N, cent, sh=1), cent=cent)
+    y = synth.add_noise(oenc.encode(sc.x_gt.astype(np.complex128), Eo).astype(np.complex64), sc.sigma,
+                        sc.noise_seed)
+    Sd, yd = ctx.upload(sc.S), ctx.upload(y)
+    recon.alternating_reconstruction(ctx, Sd, yd, sc.ky, sc.kz, sc.nEc, sc.mSt, S, N)  # warm-up
+    ctx.synchronize()
+    ctx.event(12)
+    x, T, _ = recon.alternating_reconstruction(ctx, Sd, yd, sc.ky, sc.kz, sc.nEc, sc.mSt, S, N)
+    ctx.event(13)
+    t_gpu = ctx.elapsed_ms(12, 13) * 1e-3
+    xg = x.numpy()
+    og.WORKERS = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    xo, Eo2 = osol.alternating_reconstruction(y.astype(np.complex128), Eo)
+    t_cpu = time.perf_counter() - t0
+    nr = lambda v: float(np.linalg.norm(v - sc.x_gt) / np.linalg.norm(sc.x_gt))  # noqa: E731
+    return {"workload": "64x64x64, 8 coils, 16 shots, 10 x (CG 3 + LM 1)", "gpu_s": t_gpu, "cpu_s": t_cpu,
+            "cpu_threads": og.WORKERS, "cpu_kind": "FP64 NumPy restatement (oracle), full schedule, measured",
+            "x_rel_diff": float(np.linalg.norm(xg - xo) / np.linalg.norm(xo)),
+            "T_rel_diff": float(np.linalg.norm(np.asarray(T) - Eo2.Tr) / np.linalg.norm(Eo2.Tr)),
+            "nrmse_gpu": nr(xg), "nrmse_oracle": nr(xo)}
+
+
 def alg_bytes_normal_op(N, C, S, Ns):
     """Algorithmic bytes of one normal operator (encodedecode) over S motion
     states: per state and direction 10 volume passes of 16 bytes per voxel, one
@@ -799,6 +839,7 @@ def main():
         est, thr, desc, errs = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], counts, ctx=ctx)
         out["cpu_baseline"] = {"value": est, "unit": "s", "cores": thr, "kind": "port", "sample": desc}
         out["oracle_rel_err"] = errs
+        out["config1"] = config1_run(ctx)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
