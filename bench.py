@@ -674,6 +674,8 @@ def main():
                     help="only time encode / decode / encodedecode of the scan size with SHOTS shots")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned / mixed-precision reconstructions")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch of uneven scans")
+    ap.add_argument("--n3", type=int, default=0,
+                    help="readout length for --transform-only / --operator-only (a small case for profilers)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16x3", "tf32x3"],
                     help="tensor-core contractions for --transform-only / --operator-only")
     ap.add_argument("--batch-only", action="store_true", help="only run the batch of uneven scans")
@@ -682,7 +684,9 @@ def main():
     # of mid-run: allocations of varying sizes otherwise map new memory at
     # random points of some reconstructions (0.3-0.5 s each time)
     os.environ.setdefault("DISORDER_POOL_RESERVE_GB", "80")
-    cfg = SMALL if args.small else CFG
+    cfg = dict(SMALL if args.small else CFG)
+    if args.n3:
+        cfg["N"] = (cfg["N"][0], cfg["N"][1], args.n3)
     if args.transform_only:
         return transform_only(cfg, args.transform_only, args.warmup, args.steps, args.precision)
     if args.operator_only:
