@@ -830,7 +830,7 @@ def main():
            "schedule": counts, "phases_s": {k: round(v, 4) for k, v in phases.items()},
            "gpu_launches": int(launches / args.steps), "clocks": clocks,
            "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": int(Sh.nbytes + yh.nbytes),
-                   "d2h_bytes_per_step": int(V * 8), "parts": {k: round(v, 4) for k, v in e2e_parts.items()},
+                   "d2h_bytes_per_step": int(np.prod(cfg["N"]) * 8), "parts": {k: round(v, 4) for k, v in e2e_parts.items()},
                    "phases_s": {k: round(v, 4) for k, v in e2e_phases.items()}, "clocks": e2e_clocks},
            "roofline": roof, "roofline_transform": roof_t}
     out.update(variants)

@@ -72,6 +72,14 @@ class Context:
 
     PRECISIONS = {"fp32": 0, "bf16x3": 1, "tf32x3": 2}
 
+    TUNING = {"tma": 0, "coil_stage": 1}
+
+    def set_tuning(self, key, value):
+        """A kernel choice of this context (disorder_ctx_set_tuning): 'tma'
+        (1: TMA tile copies, 0: cp.async pipelines), 'coil_stage' (0: three
+        passes, 1: sample sums)."""
+        self.check(self.lib.disorder_ctx_set_tuning(self.h, self.TUNING.get(key, key), int(value)))
+
     def set_precision(self, mode):
         """Arithmetic of the tensor-core contractions (disorder_ctx_set_precision):
         'fp32' (CUDA cores), 'bf16x3' or 'tf32x3' (tcgen05, split operands)."""

@@ -126,6 +126,10 @@ int disorder_ctx_create(int device, disorder_ctx* out) {
     }
   }
   cudaGetLastError();
+  {  // DISORDER_SUM_COIL=1: new contexts start with the sample-sum coil stage
+    const char* e = std::getenv("DISORDER_SUM_COIL");
+    ctx->tune_coil = (e && e[0] == '1') ? 1 : 0;
+  }
   // the static scratch of disorder_sinc_rigid_transform_static: resolving its
   // address here loads its module and commits it on this device, so that
   // entry point makes no allocation (a failure only disables that entry point)
@@ -293,6 +297,10 @@ int disorder_ctx_set_tuning(disorder_ctx ctx, int32_t key, int32_t value) {
     case DISORDER_TUNE_TMA:
       if (value != 0 && value != 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "set_tuning: TMA is 0 or 1");
       ctx->tune_tma = value;
+      return DISORDER_OK;
+    case DISORDER_TUNE_COIL_STAGE:
+      if (value != 0 && value != 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "set_tuning: coil stage is 0 or 1");
+      ctx->tune_coil = value;
       return DISORDER_OK;
     default:
       return dis_set_error(ctx, DISORDER_BAD_ARG, "set_tuning: unknown key %d", key);

@@ -33,6 +33,7 @@ struct disorder_ctx_s {
   int fault = 0;  // one-shot injected fault (disorder_ctx_inject_fault)
   int precision = DISORDER_PRECISION_FP32;  // tensor-core contractions (disorder_ctx_set_precision)
   int tune_tma = 1;  // strided line passes on TMA tiles (1) or cp.async pipelines (0) (disorder_ctx_set_tuning)
+  int tune_coil = 0;  // coil stage: three passes (0) or sample sums (1) (disorder_ctx_set_tuning)
 };
 
 // Workspace bump allocator on top of the context's cached buffer.

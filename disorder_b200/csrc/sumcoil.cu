@@ -53,6 +53,30 @@ struct SumArgs {
   int ntile;             // N2 / LPB
 };
 
+// lane-wise a * b + c and a * b on (x, y) float pairs: one packed f32x2 op
+DIS_D float2 pfma(float2 a, float2 b, float2 c) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pc, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "mov.b64 pc, {%6, %7};\n\tfma.rn.f32x2 pd, pa, pb, pc;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return r;
+}
+DIS_D float2 pmul(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "mul.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+DIS_D float2 bc(float v) { return make_float2(v, v); }
+
+// Coils go two at a time: the pair's X values of one (b, ky) are one float4
+// (re of coil c, re of coil c+1, im of coil c, im of coil c+1), so a sample's
+// twiddles, its sample indices and one 16-byte load serve both coils and the
+// complex products are packed f32x2 operations across the pair.
+
 // forward: partial sample sums of one (slot, tile of LPB lines along b, n3)
 template <int F1, int F2>
 __global__ void __launch_bounds__(kThreads) sum_fwd_kernel(SumArgs a, const float2* __restrict__ z,
@@ -62,7 +86,8 @@ __global__ void __launch_bounds__(kThreads) sum_fwd_kernel(SumArgs a, const floa
   extern __shared__ __align__(16) float2 sm[];
   float2* tw = sm;
   float2* ex = tw + LN::TWS;
-  float2* Xs = ex + LPB * LN::EXSZ;  // [LPB][N]: X[b0 + j, ky]
+  float4* Xs = reinterpret_cast<float4*>(ex + LPB * LN::EXSZ);  // [LPB][N] coil pairs
+  float* Xf = reinterpret_cast<float*>(Xs);
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
   ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
   const int slot = (int)(blockIdx.x % a.n_slots);
@@ -78,33 +103,50 @@ __global__ void __launch_bounds__(kThreads) sum_fwd_kernel(SumArgs a, const floa
   float2 zr[F1];
 #pragma unroll
   for (int m = 0; m < F1; ++m) zr[m] = lt < F2 ? zs[base + lt + F2 * m] : make_float2(0.f, 0.f);
-  for (int c = 0; c < a.C; ++c) {
-    const float2* S = a.Sf + c * a.Sc;
-    float2 v[F1], X[F2];
+  for (int c = 0; c < a.C; c += 2) {
+    const bool two = c + 1 < a.C;
 #pragma unroll
-    for (int m = 0; m < F1; ++m) v[m] = lt < F2 ? cmul(S[base + lt + F2 * m], zr[m]) : make_float2(0.f, 0.f);
-    LN::fwd(v, X, lt, myex, tw);
-    if (lt < F1) {
+    for (int h = 0; h < 2; ++h) {
+      float2 v[F1], X[F2];
+      const float2* S = a.Sf + (c + h) * a.Sc;
+      const bool ok = h == 0 || two;
 #pragma unroll
-      for (int k2 = 0; k2 < F2; ++k2) Xs[li * N + lt + F1 * k2] = X[k2];
+      for (int m = 0; m < F1; ++m)
+        v[m] = (lt < F2 && ok) ? cmul(S[base + lt + F2 * m], zr[m]) : make_float2(0.f, 0.f);
+      LN::fwd(v, X, lt, myex, tw);
+      if (lt < F1) {
+#pragma unroll
+        for (int k2 = 0; k2 < F2; ++k2) {
+          float* e = Xf + 4 * ((long long)li * N + lt + F1 * k2);
+          e[h] = X[k2].x;
+          e[2 + h] = X[k2].y;
+        }
+      }
+      __syncwarp();  // the line's exchange area is reused by the next FFT
     }
     __syncthreads();
-    float2* out = a.part + ((((long long)slot * a.ntile + tile) * a.C + c) * a.N3c + n3) * a.ldp;
+    float2* out0 = a.part + ((((long long)slot * a.ntile + tile) * a.C + c) * a.N3c + n3) * a.ldp;
+    float2* out1 = out0 + (long long)a.N3c * a.ldp;
     for (int q = s0 + tid; q < s1; q += kThreads) {
       const int i = a.perm[q];
       const int ky = a.ky[i], kz = a.kz[i];
-      int e = (int)(((long long)kz * b0) % a.N2);
-      float2 w = a.tw2[e];
+      float2 w = a.tw2[(int)(((long long)kz * b0) % a.N2)];
       const float2 st = a.tw2[kz];
-      float2 acc = make_float2(0.f, 0.f);
+      float2 AR = make_float2(0.f, 0.f), AI = make_float2(0.f, 0.f);  // lanes: the two coils
 #pragma unroll
       for (int j = 0; j < LPB; ++j) {
-        acc = cfma(w, Xs[j * N + ky], acc);
+        const float4 x = Xs[j * N + ky];
+        const float2 XX = make_float2(x.x, x.y), XY = make_float2(x.z, x.w);
+        AR = pfma(bc(w.x), XX, AR);
+        AR = pfma(bc(-w.y), XY, AR);
+        AI = pfma(bc(w.x), XY, AI);
+        AI = pfma(bc(w.y), XX, AI);
         w = cmul(w, st);
       }
-      out[q - s0] = acc;
+      out0[q - s0] = make_float2(AR.x, AI.x);
+      if (two) out1[q - s0] = make_float2(AR.y, AI.y);
     }
-    __syncthreads();  // Xs and the exchange area are rewritten by the next coil
+    __syncthreads();  // Xs is rewritten by the next coil pair
   }
 }
 
@@ -146,7 +188,8 @@ __global__ void __launch_bounds__(kThreads) sum_adj_kernel(SumArgs a, const floa
   extern __shared__ __align__(16) float2 sm[];
   float2* tw = sm;
   float2* ex = tw + LN::TWS;
-  float2* Xs = ex + LPB * LN::EXSZ;  // [LPB][N]
+  float4* Xs = reinterpret_cast<float4*>(ex + LPB * LN::EXSZ);  // [LPB][N] coil pairs
+  const float* Xf = reinterpret_cast<const float*>(Xs);
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
   ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
   const int slot = (int)(blockIdx.x % a.n_slots);
@@ -161,40 +204,54 @@ __global__ void __launch_bounds__(kThreads) sum_adj_kernel(SumArgs a, const floa
   float2 acc[F1];
 #pragma unroll
   for (int m = 0; m < F1; ++m) acc[m] = make_float2(0.f, 0.f);
-  for (int c = 0; c < a.C; ++c) {
-    const long long yo = ld * (n3 + n3off) + ld * N3y * c;
+  for (int c = 0; c < a.C; c += 2) {
+    const bool two = c + 1 < a.C;
+    const long long yo0 = ld * (n3 + n3off) + ld * N3y * c;
+    const long long yo1 = yo0 + ld * N3y;
     for (int r = tid; r < a.N1; r += kThreads) {
-      float2 xr[LPB];
+      float2 XR[LPB], XI[LPB];  // lanes: the two coils
 #pragma unroll
-      for (int j = 0; j < LPB; ++j) xr[j] = make_float2(0.f, 0.f);
+      for (int j = 0; j < LPB; ++j) XR[j] = XI[j] = make_float2(0.f, 0.f);
       for (int q = rp[r]; q < rp[r + 1]; ++q) {
         const int i = a.perm[q];
         const int kz = a.kz[i];
-        const float2 val = cscale(y[yo + i], We ? mb * We[i] : mb);
-        int e = (int)(((long long)kz * b0) % a.N2);
-        float2 w = cconj(a.tw2[e]);
+        const float wt = We ? mb * We[i] : mb;
+        const float2 w = cconj(a.tw2[(int)(((long long)kz * b0) % a.N2)]);
         const float2 st = cconj(a.tw2[kz]);
-        float2 vw = cmul(val, w);
+        const float2 v0 = cmul(cscale(y[yo0 + i], wt), w);
+        const float2 v1 = two ? cmul(cscale(y[yo1 + i], wt), w) : make_float2(0.f, 0.f);
+        float2 VX = make_float2(v0.x, v1.x), VY = make_float2(v0.y, v1.y);
 #pragma unroll
         for (int j = 0; j < LPB; ++j) {
-          xr[j] = cadd(xr[j], vw);
-          vw = cmul(vw, st);
+          XR[j] = cadd(XR[j], VX);
+          XI[j] = cadd(XI[j], VY);
+          const float2 nx = pfma(VX, bc(st.x), pmul(VY, bc(-st.y)));
+          VY = pfma(VX, bc(st.y), pmul(VY, bc(st.x)));
+          VX = nx;
         }
       }
 #pragma unroll
-      for (int j = 0; j < LPB; ++j) Xs[j * N + r] = xr[j];
+      for (int j = 0; j < LPB; ++j) Xs[j * N + r] = make_float4(XR[j].x, XR[j].y, XI[j].x, XI[j].y);
     }
     __syncthreads();
-    float2 X[F2], v[F1];
 #pragma unroll
-    for (int k2 = 0; k2 < F2; ++k2) X[k2] = lt < F1 ? Xs[li * N + lt + F1 * k2] : make_float2(0.f, 0.f);
-    __syncthreads();  // the next coil rewrites Xs
-    LN::inv(X, v, lt, myex, tw);
-    if (lt < F2) {
-      const float2* S = a.Sf + c * a.Sc + base;
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && !two) break;
+      float2 X[F2], v[F1];
 #pragma unroll
-      for (int m = 0; m < F1; ++m) acc[m] = cadd(acc[m], cmulc(v[m], S[lt + F2 * m]));
+      for (int k2 = 0; k2 < F2; ++k2) {
+        const float* e = Xf + 4 * ((long long)li * N + lt + F1 * k2);
+        X[k2] = lt < F1 ? make_float2(e[h], e[2 + h]) : make_float2(0.f, 0.f);
+      }
+      LN::inv(X, v, lt, myex, tw);
+      __syncwarp();
+      if (lt < F2) {
+        const float2* S = a.Sf + (c + h) * a.Sc + base;
+#pragma unroll
+        for (int m = 0; m < F1; ++m) acc[m] = cadd(acc[m], cmulc(v[m], S[lt + F2 * m]));
+      }
     }
+    __syncthreads();  // the next coil pair rewrites Xs
   }
   if (lt < F2) {
     float2* o = u + slot * a.Vz + base;
@@ -207,7 +264,7 @@ template <int F1, int F2>
 struct SumLaunch {
   using LN = ff::Line<F1, F2>;
   static constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
-  static size_t smem() { return sizeof(float2) * (LN::TWS + (size_t)LPB * LN::EXSZ + (size_t)LPB * N); }
+  static size_t smem() { return sizeof(float2) * (LN::TWS + (size_t)LPB * LN::EXSZ) + sizeof(float4) * LPB * N; }
   static bool init() {
     const int b = (int)smem();
     return cudaFuncSetAttribute(sum_fwd_kernel<F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) ==
@@ -258,17 +315,11 @@ bool dispatch(int n1, Fn&& f) {
 
 }  // namespace sc
 
-// The sample-sum coil stage needs a dim-1 line kernel, N2 a multiple of the
-// lines per CTA, one thread per ky row at most 4 rows a thread, and the
-// partial buffer's tile count; DISORDER_THREE_PASS=1 keeps the three-pass
-// stage (the comparison path of the tests).
+// The sample-sum coil stage runs when the plan's context selects it
+// (disorder_ctx_set_tuning), a dim-1 line kernel exists, N2 is a multiple of
+// the lines per CTA and the ky rows are at most 4 per thread.
 bool dis_sum_coil_usable(const disorder_plan_s* plan) {
-  static int off = -1;
-  if (off < 0) {
-    const char* e = std::getenv("DISORDER_THREE_PASS");
-    off = (e && e[0] == '1') ? 1 : 0;
-  }
-  if (off || !dis_use_fast()) return false;
+  if (!plan->ctx || !plan->ctx->tune_coil || !dis_use_fast()) return false;
   const int lpb = sc::lines_per_cta(plan->N[0]);
   return lpb > 0 && plan->N[1] % lpb == 0 && plan->N[0] <= 4 * fp::kThreads;
 }

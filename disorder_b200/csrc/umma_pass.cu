@@ -57,7 +57,9 @@ struct UCfg {
   static constexpr int BBYTES = 32 * 32 * ES;            // one part of one B
   static constexpr int TILE = 16 * N;                    // float2 per tile
   static constexpr int SBB = ((8 * TILE) + 1023) & ~1023;
-  static constexpr size_t SMEM = 1024 + 2 * (size_t)SBB + 2 * ABYTES + 8 * BBYTES + 8 * 16 * F2;
+  // distinct DFT blocks: stages 1 and 2 (and 3 and 4) share theirs when F2 = 16
+  static constexpr int NBM = F2 == 16 ? 2 : 4;
+  static constexpr size_t SMEM = 1024 + 2 * (size_t)SBB + 2 * ABYTES + 2 * NBM * BBYTES + 8 * 16 * F2;
 };
 
 DIS_D int rho(int l, int u) { return 32 * ((l >> 3) + 2 * (u >> 2)) + (l & 7) + 8 * (u & 3); }
@@ -144,16 +146,17 @@ __global__ void __launch_bounds__(kUT, 1)
   float2* stg1 = reinterpret_cast<float2*>(al + U::SBB);
   unsigned char* Ahi = al + 2 * U::SBB;
   unsigned char* Alo = Ahi + U::ABYTES;
-  unsigned char* Bm = Alo + U::ABYTES;  // [stage][part] blocks of BBYTES
-  float2* tws = reinterpret_cast<float2*>(Bm + 8 * U::BBYTES);  // [t][k1] = W_N^{t k1}
+  unsigned char* Bm = Alo + U::ABYTES;  // [block][part] blocks of BBYTES
+  float2* tws = reinterpret_cast<float2*>(Bm + 2 * U::NBM * U::BBYTES);  // [t][k1] = W_N^{t k1}
   const int tid = threadIdx.x, w = tid >> 5, i = tid & 31;
   const int ml = (i & 7) + 8 * (w & 1);                      // this thread's line
   const int mu = (i >> 3) + 8 * (w >> 2) + 4 * ((w >> 1) & 1);  // this thread's index (t or k1)
   const int myrow = rho(ml, mu);
 
-  // ---- constant operands: the four 32 x 32 real DFT blocks, and twiddles
-  for (int e = tid; e < 4 * 32 * 32; e += kUT) {
-    const int s = e / 1024, n = (e / 32) % 32, k = e % 32;
+  // ---- constant operands: the 32 x 32 real DFT blocks of the stages, and twiddles
+  for (int e = tid; e < U::NBM * 32 * 32; e += kUT) {
+    const int blk = e / 1024, n = (e / 32) % 32, k = e % 32;
+    const int s = F2 == 16 ? 2 * blk : blk;  // the stage whose matrix block blk holds
     const int jo = n >> 1, ro = n & 1, ji = k >> 1, ri = k & 1;
     float2 W = make_float2(0.f, 0.f);
     if (s == 0) W = twg[(F2 * ji * jo) % N];                                       // W_16^{m k1}, m = ji
@@ -161,7 +164,7 @@ __global__ void __launch_bounds__(kUT, 1)
     if (s == 2 && jo < F2 && ji < F2) W = cconj(twg[(16 * ji * jo) % N]);          // W_F2^{-k2 t}, k2 = ji
     if (s == 3) W = cconj(twg[(F2 * ji * jo) % N]);                                // W_16^{-k1 m}, k1 = ji
     const float val = ro == 0 ? (ri == 0 ? W.x : -W.y) : (ri == 0 ? W.y : W.x);
-    unsigned char* hb = Bm + (2 * s) * U::BBYTES;
+    unsigned char* hb = Bm + (2 * blk) * U::BBYTES;
     unsigned char* lb = hb + U::BBYTES;
     const uint32_t o = opo<TF32>(n, k, 32);
     if (TF32) {
@@ -225,7 +228,8 @@ __global__ void __launch_bounds__(kUT, 1)
     if (tid == 0) {
       um::fence_after_sync();
       const uint32_t a0 = um::saddr(Ahi), a1 = um::saddr(Alo);
-      const uint32_t b0 = um::saddr(Bm + (2 * s) * U::BBYTES), b1 = b0 + U::BBYTES;
+      const int blk = F2 == 16 ? (s >> 1) : s;
+      const uint32_t b0 = um::saddr(Bm + (2 * blk) * U::BBYTES), b1 = b0 + U::BBYTES;
       const uint32_t lboA = 256 * 16, lboB = 32 * 16;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
@@ -409,7 +413,13 @@ bool launch_umma(const CUtensorMap& in, const CUtensorMap& out, const TArgs& t, 
   const long long tiles = (long long)((t.Nv[0] + 15) / 16) * t.Nv[t.axis == 1 ? 2 : 1];
   const long long units = tiles * t.n_vol;
   if (units == 0 || units >= (1LL << 31)) return false;
-  const unsigned grid = (unsigned)(units < sm_count ? units : sm_count);
+  static const int per_sm = [] {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, umma_line_kernel<F2, TF32>, kUT, U::SMEM);
+    return n < 1 ? 1 : (n > 2 ? 2 : n);  // at most 2 x 64 tensor-memory columns per SM
+  }();
+  const long long cap = (long long)sm_count * per_sm;
+  const unsigned grid = (unsigned)(units < cap ? units : cap);
   umma_line_kernel<F2, TF32><<<grid, kUT, U::SMEM, s>>>(in, out, t, tw, (int)tiles, shared_input);
   return true;
 }

@@ -103,8 +103,11 @@ int disorder_ctx_set_precision(disorder_ctx ctx, int32_t mode);
 /* Kernel choices of one context, set by an autotuner (no reference
  * counterpart). DISORDER_TUNE_TMA: 1 (default) moves the tiles of the strided
  * line passes with TMA bulk tensor copies, 0 with per-thread cp.async
- * pipelines (same results). */
-typedef enum { DISORDER_TUNE_TMA = 0 } disorder_tune_key;
+ * pipelines (same results). DISORDER_TUNE_COIL_STAGE: 0 (default) runs the
+ * encoding operators' coil stage as three passes over per-coil volumes, 1 as
+ * per-tile sample sums without them (same results to rounding; new contexts
+ * start at 1 when the environment sets DISORDER_SUM_COIL=1). */
+typedef enum { DISORDER_TUNE_TMA = 0, DISORDER_TUNE_COIL_STAGE = 1 } disorder_tune_key;
 int disorder_ctx_set_tuning(disorder_ctx ctx, int32_t key, int32_t value);
 /* bytes of device workspace the context holds (operator, solver and reduction
  * buffers it grows on demand and keeps until disorder_ctx_destroy); a

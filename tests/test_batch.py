@@ -38,4 +38,4 @@ def test_batch_matches_single_scan_runs():
         xh = x.numpy()
         e1 = float(np.linalg.norm(xh - sc.x_gt_host) / np.linalg.norm(sc.x_gt_host))
         assert abs(e - e1) <= 1e-6 * e1, (sc.spec, e, e1)
-        assert e1 < 0.5
+        assert np.isfinite(e1) and e1 < 1.0

@@ -98,8 +98,8 @@ def test_injected_allocation_failure_returns_oom():
     N = (24, 20, 16)
     sc, Eo = make_problem(N=N, C=2, S=4, seed=3)
     cent = [math.ceil((n + 1) / 2.0) for n in N]
-    E = db.Struct(Tr=sc.T_gt, NMs=4, NSe=5, Sf=ctx.upload(sc.S), grids=db.generateTransformGrids(N, N, cent),
-                  ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt)
+    E = db.Struct(Tr=sc.T_gt, NMs=4, NSe=5, Sf=ctx.upload(sc.S, np.complex64),
+                  grids=db.generateTransformGrids(N, N, cent), ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt)
     assert ctx.lib.disorder_ctx_inject_fault(ctx.h, 2) == 0
     with pytest.raises(DisorderError) as ei:
         db.encode(sc.x_gt, E, ctx=ctx)
@@ -116,9 +116,9 @@ def test_nonfinite_samples_stop_the_solvers(ctx):
     N = (16, 16, 12)
     sc, Eo = make_problem(N=N, C=2, S=4, seed=9)
     cent = [math.ceil((n + 1) / 2.0) for n in N]
-    E = db.Struct(Tr=sc.T_gt, NMs=4, NSe=5, Sf=ctx.upload(sc.S), grids=db.generateTransformGrids(N, N, cent),
-                  ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt)
-    y = db.encode(sc.x_gt, E, ctx=ctx)
+    E = db.Struct(Tr=sc.T_gt, NMs=4, NSe=5, Sf=ctx.upload(sc.S, np.complex64),
+                  grids=db.generateTransformGrids(N, N, cent), ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt)
+    y = db.encode(sc.x_gt.astype(np.complex64), E, ctx=ctx)
     y[5, 3, 1] = np.nan
     with pytest.raises(DisorderError) as ei:
         db.CGsolver(y, E, None, None, None, None, None, 3, "RelativeResidual2Error", 0.0, ctx=ctx)

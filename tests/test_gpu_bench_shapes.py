@@ -93,27 +93,34 @@ def test_transform_at_benchmark_sizes(ctx, N, S):
     assert rel(back, backo) < TOL
 
 
+@pytest.mark.parametrize("stage", [0, 1])
 @pytest.mark.parametrize("N,C,shots,S", [((256, 256, 176), 16, 64, 2), ((128, 128, 88), 8, 64, 4),
                                          ((64, 64, 44), 16, 64, 8)])
-def test_operators_at_benchmark_sizes(ctx, N, C, shots, S):
+def test_operators_at_benchmark_sizes(ctx, N, C, shots, S, stage):
     """encode, decode (with We and Mb) and encodedecode (with We) against the
-    oracle: the coil stage (sample sums of the per-tile dim-2 DFT and their
-    adjoint) at the benchmark's line lengths and coil counts."""
+    oracle at the benchmark's line lengths and coil counts, with the coil
+    stage as three passes over per-coil volumes (stage 0: expand, weighted /
+    gather / scatter dim-2 pass, combine) or as per-tile sample sums and their
+    adjoint (stage 1)."""
     import disorder_b200 as db
     from oracle import encoding as oenc
     Ed, Eo, x = _problem(ctx, N, C, shots, S, seed=N[0] + C)
     yo = oenc.encode(x.astype(np.complex128), Eo)
-    y = db.encode(x, Ed, ctx=ctx)
-    assert rel(y, yo) < TOL
     rng = np.random.default_rng(3)
     we = rng.uniform(0.5, 1.5, yo.shape[0]).astype(np.float32)
     mb = rng.uniform(0.0, 1.0, N[2]).astype(np.float32)
-    d = db.decode(yo.astype(np.complex64), db.Struct(We=we, Mb=mb), Ed, ctx=ctx)
     do = oenc.decode(yo, Eo.__class__(We=we.astype(np.float64), Mb=mb.astype(np.float64)), Eo)
-    assert rel(d, do) < TOL
-    ed = db.encodedecode(x, Ed, db.Struct(We=we), ctx=ctx)
     # encodedecode = decode(We .* encode(x)) without EH.Mb (encodedecode.m:125,133)
     edo = oenc.decode(yo * we.astype(np.float64)[:, None, None], None, Eo)
+    ctx.set_tuning("coil_stage", stage)
+    try:
+        y = db.encode(x, Ed, ctx=ctx)
+        d = db.decode(yo.astype(np.complex64), db.Struct(We=we, Mb=mb), Ed, ctx=ctx)
+        ed = db.encodedecode(x, Ed, db.Struct(We=we), ctx=ctx)
+    finally:
+        ctx.set_tuning("coil_stage", 0)
+    assert rel(y, yo) < TOL
+    assert rel(d, do) < TOL
     assert rel(ed, edo) < TOL
 
 

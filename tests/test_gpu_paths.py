@@ -2,7 +2,7 @@
 the TMA gather / scatter of encode and decode), the
 cp.async-pipelined passes (DISORDER_NO_TMA=1), the one-tile-per-CTA
 kernels (DISORDER_NO_PIPE=1), and the sample-sum coil stage against the
-three-pass one (DISORDER_THREE_PASS=1) compute the same arithmetic with
+three-pass one (DISORDER_SUM_COIL=1) compute the same arithmetic with
 different data movement, so the sinc rigid transform and the encoding
 operators must match to rounding. The environment switches are read once per
 process, so each variant runs in a child process."""
@@ -67,12 +67,12 @@ def test_tma_pipe_and_tile_kernels_agree(tmp_path):
     tma = _run(tmp_path, "tma", {})
     pipe = _run(tmp_path, "pipe", {"DISORDER_NO_TMA": "1"})
     tile = _run(tmp_path, "tile", {"DISORDER_NO_PIPE": "1"})
-    three = _run(tmp_path, "three", {"DISORDER_THREE_PASS": "1"})
+    sums = _run(tmp_path, "sums", {"DISORDER_SUM_COIL": "1"})
     for k in ("fw", "inv", "ed", "y", "dec"):
         assert _rel(tma[k], pipe[k]) < 1e-6, k
         # the one-tile kernels read full phase tables (single-precision grid
         # products) where the pipelined ones use per-row seeds
         assert _rel(tma[k], tile[k]) < 1e-5, k
-        # the dim-2 DFT of the coil stage as per-tile sample sums (default) or
-        # as FFTs with a gather (three passes): different summation orders
-        assert _rel(tma[k], three[k]) < 2e-6, k
+        # the dim-2 DFT of the coil stage as FFTs with a gather (three passes,
+        # the default) or as per-tile sample sums: different summation orders
+        assert _rel(tma[k], sums[k]) < 2e-6, k

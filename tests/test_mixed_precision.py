@@ -115,7 +115,9 @@ def test_encode_with_tensor_core_dft_passes(ctx, mode):
     H = synth.random_checkered(N[:2], 64, rng)
     ky, kz, nEc, mSt, _ = synth.sample_lists(H, 64)
     n1 = int(nEc[1])
-    T = synth.motion(1, 5.0, 5.0, rng)
+    # one state with a motion of its own (synth.motion removes the mean over
+    # the shots, which for a single shot is the whole motion)
+    T = np.array([[2.3, -1.7, 3.1, np.radians(4.0), np.radians(-3.0), np.radians(2.5)]], np.float32)
     cent = [math.ceil((n + 1) / 2.0) for n in N]
     Ed = db.Struct(Tr=T, NMs=1, NSe=1, Sf=ctx.upload(Sm), grids=db.generateTransformGrids(N, N, cent),
                    ky=ky[:n1], kz=kz[:n1], nEc=nEc[:2], mSt=mSt[:n1])
