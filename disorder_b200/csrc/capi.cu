@@ -337,6 +337,7 @@ int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* g, const di
   if (!g || !smp || !out) return dis_set_error(ctx, DISORDER_BAD_ARG, "plan: null argument");
   *out = nullptr;
   DEV_GUARD(ctx);
+  cudaGetLastError();  // the checks below read each call's own status, not an earlier one
   disorder_plan_s* p = new disorder_plan_s();
   p->ctx = ctx;
   auto fail = [&](int st) {
@@ -376,8 +377,9 @@ int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* g, const di
     if (cudaMalloc(&p->d_kG[m], sizeof(float) * p->N[m]) != cudaSuccess ||
         cudaMalloc(&p->d_rG[m], sizeof(float) * p->N[m]) != cudaSuccess)
       return fail(dis_set_error(ctx, DISORDER_OOM, "plan: grid allocation"));
-    cudaMemcpy(p->d_kG[m], p->kG[m].data(), sizeof(float) * p->N[m], cudaMemcpyHostToDevice);
-    cudaMemcpy(p->d_rG[m], p->rG[m].data(), sizeof(float) * p->N[m], cudaMemcpyHostToDevice);
+    if (cudaMemcpy(p->d_kG[m], p->kG[m].data(), sizeof(float) * p->N[m], cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->d_rG[m], p->rG[m].data(), sizeof(float) * p->N[m], cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(dis_set_error(ctx, DISORDER_CUDA_ERR, "plan: grid upload: %s", cudaGetErrorString(cudaGetLastError())));
     // twiddles exp(-2 pi i j / N) in double precision, rounded to single
     std::vector<float2> tw(p->N[m]);
     for (int j = 0; j < p->N[m]; ++j) {
@@ -386,7 +388,8 @@ int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* g, const di
     }
     if (cudaMalloc(&p->d_tw[m], sizeof(float2) * p->N[m]) != cudaSuccess)
       return fail(dis_set_error(ctx, DISORDER_OOM, "plan: twiddle allocation"));
-    cudaMemcpy(p->d_tw[m], tw.data(), sizeof(float2) * p->N[m], cudaMemcpyHostToDevice);
+    if (cudaMemcpy(p->d_tw[m], tw.data(), sizeof(float2) * p->N[m], cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(dis_set_error(ctx, DISORDER_CUDA_ERR, "plan: twiddle upload: %s", cudaGetErrorString(cudaGetLastError())));
   }
   // sampling
   if (smp->n_seg < 0 || smp->n_mot < 0 || smp->n_mot > smp->n_seg || !smp->seg_offsets)
@@ -418,16 +421,15 @@ int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* g, const di
   }
   auto up = [&](void** d, const void* h, size_t bytes) -> bool {
     if (cudaMalloc(d, std::max<size_t>(bytes, 4)) != cudaSuccess) return false;
-    if (bytes) cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice);
-    return true;
+    return !bytes || cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
   };
   if (!up((void**)&p->d_ky, smp->ky, sizeof(int) * ns) || !up((void**)&p->d_kz, smp->kz, sizeof(int) * ns) ||
       !up((void**)&p->d_seg_of, segof.data(), sizeof(int) * ns) ||
       !up((void**)&p->d_perm, perm.data(), sizeof(int) * ns) ||
       !up((void**)&p->d_rowptr, rowptr.data(), sizeof(int) * rowptr.size()) ||
       !up((void**)&p->d_seg_off, p->seg_off.data(), sizeof(long long) * p->seg_off.size()))
-    return fail(dis_set_error(ctx, DISORDER_OOM, "plan: sample table allocation"));
-  if (cudaGetLastError() != cudaSuccess) return fail(dis_set_error(ctx, DISORDER_CUDA_ERR, "plan: upload failed"));
+    return fail(dis_set_error(ctx, DISORDER_OOM, "plan: sample table allocation or upload: %s",
+                              cudaGetErrorString(cudaGetLastError())));
   *out = p;
   return DISORDER_OK;
 }

@@ -313,6 +313,7 @@ struct PipeLaunch {
   static void prep(Occ& o) {
     auto k = pipe_kernel<F1, F2, ACC, SEED>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
+    cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm[(ACC ? 1 : 0) + (SEED ? 2 : 0)], k, kThreads, P::SMEM);
   }
   static Occ init() {
@@ -475,6 +476,8 @@ struct WPipeLaunch {
   static Occ init() {
     Occ o;
     cudaFuncSetAttribute(wpipe_kernel<F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
+    cudaFuncSetAttribute(wpipe_kernel<F1, F2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, wpipe_kernel<F1, F2>, kThreads, P::SMEM);
     int dev = 0;
     cudaGetDevice(&dev);

@@ -267,9 +267,15 @@ struct SumLaunch {
   static size_t smem() { return sizeof(float2) * (LN::TWS + (size_t)LPB * LN::EXSZ) + sizeof(float4) * LPB * N; }
   static bool init() {
     const int b = (int)smem();
-    return cudaFuncSetAttribute(sum_fwd_kernel<F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) ==
-               cudaSuccess &&
-           cudaFuncSetAttribute(sum_adj_kernel<F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) == cudaSuccess;
+    const int co = (int)cudaSharedmemCarveoutMaxShared;  // two CTAs per SM
+    const bool r =
+        cudaFuncSetAttribute(sum_fwd_kernel<F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) == cudaSuccess &&
+        cudaFuncSetAttribute(sum_adj_kernel<F1, F2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) == cudaSuccess &&
+        cudaFuncSetAttribute(sum_fwd_kernel<F1, F2>, cudaFuncAttributePreferredSharedMemoryCarveout, co) ==
+            cudaSuccess &&
+        cudaFuncSetAttribute(sum_adj_kernel<F1, F2>, cudaFuncAttributePreferredSharedMemoryCarveout, co) == cudaSuccess;
+    cudaGetLastError();
+    return r;
   }
   static bool fwd(const SumArgs& a, const float2* z, const float2* tw, cudaStream_t s) {
     static const bool ok = init();

@@ -360,6 +360,9 @@ struct TmaLaunch {
   template <int KIND>
   static void prep(Occ& o) {
     cudaFuncSetAttribute(tma_kernel<F1, F2, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
+    // the largest carveout, so the persistent grid's CTAs per SM are all resident
+    cudaFuncSetAttribute(tma_kernel<F1, F2, KIND>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm[KIND], tma_kernel<F1, F2, KIND>, kThreads, P::SMEM);
   }
   static Occ init() {

@@ -406,8 +406,13 @@ bool launch_umma(const CUtensorMap& in, const CUtensorMap& out, const TArgs& t, 
                  int sm_count, cudaStream_t s) {
   using U = UCfg<F2, TF32>;
   static const bool ok = [] {
-    return cudaFuncSetAttribute(umma_line_kernel<F2, TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)U::SMEM) == cudaSuccess;
+    // the largest shared-memory carveout, so that two CTAs fit on an SM
+    const bool r = cudaFuncSetAttribute(umma_line_kernel<F2, TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)U::SMEM) == cudaSuccess &&
+                   cudaFuncSetAttribute(umma_line_kernel<F2, TF32>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared) == cudaSuccess;
+    cudaGetLastError();
+    return r;
   }();
   if (!ok) return false;
   const long long tiles = (long long)((t.Nv[0] + 15) / 16) * t.Nv[t.axis == 1 ? 2 : 1];

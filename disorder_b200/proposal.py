@@ -195,10 +195,14 @@ def restrict(T):
     return T
 
 
-def propose_step(net, y, E, x, nF=None, ctx=None):
+def propose_step(net, y, E, x, nF=None, ctx=None, refresh=None):
     """One proposal round for the states not yet converged: returns (E with
     the accepted proposals applied to Tr, accepted mask). A proposal is kept
-    only where it lowers the state's energy."""
+    only where it lowers the state's energy. The energies are compared at the
+    current image x, or, with refresh = (EH, A) of the image update, at x
+    refreshed by one CG iteration (CGsolver.m) with the proposed motion: the
+    current image is a blur of all shots' poses, which favours the average
+    pose over each shot's own."""
     ctx = ctx or net.ctx
     act = ~np.asarray(E.cT, bool)
     if not act.any():
@@ -208,8 +212,14 @@ def propose_step(net, y, E, x, nF=None, ctx=None):
     T1 = T0.copy()
     T1[act] = T0[act] + dT[act]
     T1 = restrict(T1)
-    En0 = state_energies(y, E, x, nF, ctx=ctx)
-    En1 = state_energies(y, E.copy(Tr=T1), x, nF, ctx=ctx)
+    xg = x
+    if refresh is not None:
+        EH, A = refresh
+        xg = ctx.empty(x.shape)
+        ctx.check(ctx.lib.disorder_memcpy_d2d(ctx.h, xg.ptr, x.ptr, x.nbytes))
+        xg, _, _ = api.CGsolver(y, E.copy(Tr=T1), EH, A, None, None, xg, 1, "RelativeResidual2Error", 0.0, ctx=ctx)
+    En0 = state_energies(y, E, xg, nF, ctx=ctx)
+    En1 = state_energies(y, E.copy(Tr=T1), xg, nF, ctx=ctx)
     acc = act & (En1 < En0)
     T = T0.copy()
     T[acc] = T1[acc]
@@ -287,7 +297,7 @@ def motion_error(T, T_true):
     return float(np.abs(d[:, :3]).max()), float(np.degrees(np.abs(d[:, 3:]).max()))
 
 
-def level_run(ctx, sim, net=None, n_outer=9, winit=1e-3, traLimXT=(0.05, 0.02), resIso=None):
+def level_run(ctx, sim, net=None, n_outer=9, winit=1e-3, traLimXT=(0.05, 0.02), resIso=None, refresh=False):
     """Motion estimation on one level as the driver runs it (solveXT.m:379-388,
     431, 507): outer iterations of one CG iteration and one LM step, with
     the proposal round before the LM step when net is given. Returns a dict
@@ -313,7 +323,8 @@ def level_run(ctx, sim, net=None, n_outer=9, winit=1e-3, traLimXT=(0.05, 0.02), 
         x, _, _ = api.CGsolver(sim.y, E, api.Struct(Mbe=sim.Mbe), api.Struct(Se=sim.Se), None, None, x, 1,
                                "RelativeResidual2Error", 0.0, ctx=ctx)
         if net is not None:
-            E, acc = propose_step(net, sim.y, E, x, sim.nF, ctx=ctx)
+            E, acc = propose_step(net, sim.y, E, x, sim.nF, ctx=ctx,
+                                  refresh=(api.Struct(Mbe=sim.Mbe), api.Struct(Se=sim.Se)) if refresh else None)
             out["accepted"] += int(acc.sum())
         out["lm_states"] += int(np.sum(~np.asarray(E.cT, bool)))
         E = api.LMsolver(sim.y, E, x, ctx=ctx)
@@ -328,7 +339,7 @@ def level_run(ctx, sim, net=None, n_outer=9, winit=1e-3, traLimXT=(0.05, 0.02), 
     return out
 
 
-def compare(ctx, net, n_scans=4, seed=9000, n_outer=9, max_deg=5.0, max_vox=5.0):
+def compare(ctx, net, n_scans=4, seed=9000, n_outer=9, max_deg=5.0, max_vox=5.0, refresh=False):
     """level_run with and without the proposal on n_scans simulated scans with
     config-2 motion (U(-5, 5) deg / voxels). Returns (plain runs, learned runs)."""
     rng = np.random.default_rng(seed)
@@ -336,7 +347,7 @@ def compare(ctx, net, n_scans=4, seed=9000, n_outer=9, max_deg=5.0, max_vox=5.0)
     for _ in range(n_scans):
         sim = simulate_level(ctx, rng, max_deg=max_deg, max_vox=max_vox)
         plain.append(level_run(ctx, sim, None, n_outer))
-        learned.append(level_run(ctx, sim, net, n_outer))
+        learned.append(level_run(ctx, sim, net, n_outer, refresh=refresh))
     return plain, learned
 
 
