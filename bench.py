@@ -270,10 +270,11 @@ def cpu_estimate(N, n_states, C, counts, ctx=None):
 
 
 def oracle_check(ctx, x, Eo, ed_oracle):
-    """Relative L2 error of the library (FP32 on the GPU) against the FP64
-    oracle for one motion state at full size: forward transform, encode,
-    decode and encodedecode of the same inputs (state 0 of the sampled
-    problem, its samples only)."""
+    """Relative L2 error of the library on the GPU against the FP64 oracle
+    for one motion state at full size: forward transform, encode, decode and
+    encodedecode of the same inputs (state 0 of the sampled problem, its
+    samples only), with the DFT passes on CUDA cores (fp32) and on the tensor
+    cores (bf16x3, tf32x3)."""
     import disorder_b200 as db
     from oracle import encoding as oenc
     from oracle.transform import precomputeFactorsSincRigidTransform as opf
@@ -294,13 +295,19 @@ def oracle_check(ctx, x, Eo, ed_oracle):
 
     out = {"workload": "%s, %d coils, 1 state of %d samples" % ("x".join(map(str, N)), Eo.Sf.shape[3], n1 - n0)}
     et, _ = db.precomputeFactorsSincRigidTransform(Ed.grids, T, 1)
-    zt, _ = db.sincRigidTransform(x32, et, 1, ctx=ctx)
     oet, _ = opf(Eo.grids, T, 1, 0)
-    out["transform"] = rel(zt[..., 0], ost(x.reshape(N + (1, 1)), oet, 1)[:, :, :, 0, 0])
+    zo = ost(x.reshape(N + (1, 1)), oet, 1)[:, :, :, 0, 0]
     yo = oenc.encode(x, Es)
-    out["encode"] = rel(db.encode(x32, Ed, ctx=ctx), yo)
-    out["decode"] = rel(db.decode(yo.astype(np.complex64), None, Ed, ctx=ctx), oenc.decode(yo, None, Es))
-    out["encodedecode"] = rel(db.encodedecode(x32, Ed, None, ctx=ctx), ed_oracle)
+    do = oenc.decode(yo, None, Es)
+    for prec in ("fp32", "bf16x3", "tf32x3"):
+        ctx.set_precision(prec)
+        try:
+            zt, _ = db.sincRigidTransform(x32, et, 1, ctx=ctx)
+            out[prec] = {"transform": rel(zt[..., 0], zo), "encode": rel(db.encode(x32, Ed, ctx=ctx), yo),
+                         "decode": rel(db.decode(yo.astype(np.complex64), None, Ed, ctx=ctx), do),
+                         "encodedecode": rel(db.encodedecode(x32, Ed, None, ctx=ctx), ed_oracle)}
+        finally:
+            ctx.set_precision("fp32")
     return out
 
 
@@ -545,7 +552,7 @@ def batch_arm(n_scans=32, seed=4000, workers=(1, 2, 4)):
 
 
 # ---------------------------------------------------------------- rooflines
-def normal_operator_roofline(ctx, cfg, peak, pkind, reps=5):
+def normal_operator_roofline(ctx, cfg, peak, pkind, reps=5, precision="fp32"):
     """One normal operator (encodedecode) of a random volume of the scan size
     with the kept coil count and all shots (random-checkered sampling, random
     motion) through the C ABI with preallocated buffers; CUDA events on the
@@ -575,19 +582,24 @@ def normal_operator_roofline(ctx, cfg, peak, pkind, reps=5):
     def call():
         ctx.check(ctx.lib.disorder_encodedecode(ctx.h, plan.h, xd.ptr, Sd.ptr, C, Tp, None, out.ptr))
 
-    call()
-    ctx.synchronize()
-    ctx.event(4)
-    for _ in range(reps):
+    ctx.set_precision(precision)
+    try:
         call()
-    ctx.event(5)
+        ctx.synchronize()
+        ctx.event(4)
+        for _ in range(reps):
+            call()
+        ctx.event(5)
+    finally:
+        ctx.set_precision("fp32")
     t = ctx.elapsed_ms(4, 5) / reps
     Ns = int(np.max(np.diff(nEc)[:S]))
     alg = alg_bytes_normal_op(N, C, S, Ns)
     achieved = alg / (t * 1e-3) / 1e9
     del Sd, xd, out
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": TRAFFIC_NORMAL_OP, "peak_kind": pkind, "bytes_per_launch": alg, "ms": t,
+            "traffic": TRAFFIC_NORMAL_OP if precision == "fp32" else None, "peak_kind": pkind,
+            "bytes_per_launch": alg, "ms": t, "precision": precision,
             "kernel": "normal operator encodedecode (transform line passes, coil expand, weighted dim-2 pass, "
                       "coil combine, inverse transform with state sum)",
             "timing": "one encodedecode of %s, %d coils, %d shots through the C ABI, CUDA events, mean of %d; "
@@ -672,7 +684,10 @@ def main():
                     help="only time the sinc rigid transform of the scan size with STATES states")
     ap.add_argument("--operator-only", type=int, default=0, metavar="SHOTS",
                     help="only time encode / decode / encodedecode of the scan size with SHOTS shots")
-    ap.add_argument("--no-learned", action="store_true", help="skip the learned / mixed-precision reconstructions")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the single-run learned-only and mixed-only reconstructions")
+    ap.add_argument("--plain", action="store_true",
+                    help="headline = the plain FP32 method (no proposal, no tensor-core passes)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch of uneven scans")
     ap.add_argument("--n3", type=int, default=0,
                     help="readout length for --transform-only / --operator-only (a small case for profilers)")
@@ -726,46 +741,76 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     import disorder_b200 as db
-    from disorder_b200 import recon
+    from disorder_b200 import proposal, recon
     ctx = db.Context(local)
     cfg_r = dict(cfg)
     cfg_r["seed"] = replica_seed(cfg["seed"], rank)
     sc = build_scan(ctx, cfg_r)
+    net = None
+    if not args.plain and os.path.exists(proposal.WEIGHTS):
+        net = proposal.MotionNet.load(ctx, proposal.WEIGHTS)
+    head_prec = "fp32" if args.plain else "bf16x3"
 
-    def one(S, y):
-        return recon.aligned_reconstruction(ctx, S, y, sc.H, cfg["shots"], cfg["N"], perc=cfg["coils_kept"])
+    def arm(learned, precision):
+        """W untimed and K timed reconstructions (CUDA events on the library's
+        stream, barrier before and after, max over ranks)."""
+        pnet = net if learned else None
 
-    for _ in range(args.warmup):
-        x, T, log = one(sc.S, sc.y)
-    ctx.synchronize()
-    barrier(world)
-    clk = NvmlClockSampler(local)
-    clk.start()
-    l0 = ctx.launches
-    if args.profile_region:
-        import torch
-        torch.cuda.profiler.start()
-    ctx.event(0)
-    logs = []
-    for _ in range(args.steps):
-        x, T, log = one(sc.S, sc.y)
-        logs.append(log)
-    ctx.event(1)
-    if args.profile_region:
-        ctx.synchronize()
-        torch.cuda.profiler.stop()
-    ms_total = ctx.elapsed_ms(0, 1)
-    launches = ctx.launches - l0
-    clocks = clk.stop()
-    barrier(world)
-    ms = ms_total / args.steps
-    if world > 1:
-        ms = ranks_max(ms, "cuda:%d" % local)
-    err = nrmse(ctx, x, sc.x_gt_host)
-    motion_err = float(np.max(np.abs(T - sc.T_gt)[:, :3])), float(np.degrees(np.max(np.abs(T - sc.T_gt)[:, 3:])))
-    phases = phase_split(logs[-1])
-    counts = {"outer": [sum(1 for e in logs[-1].events if e["step"] == "lm" and e["level"] == lv) for lv in (0, 1)],
-              "cg_final": sum(e["iters"] for e in logs[-1].events if e["step"] == "cg" and e["level"] == 2)}
+        def one(S, y):
+            return recon.aligned_reconstruction(ctx, S, y, sc.H, cfg["shots"], cfg["N"], perc=cfg["coils_kept"],
+                                                proposal=pnet)
+
+        ctx.set_precision(precision)
+        try:
+            for _ in range(args.warmup):
+                one(sc.S, sc.y)
+            ctx.synchronize()
+            barrier(world)
+            clk = NvmlClockSampler(local)
+            clk.start()
+            l0 = ctx.launches
+            if args.profile_region:
+                import torch
+                torch.cuda.profiler.start()
+            ctx.event(0)
+            logs = []
+            for _ in range(args.steps):
+                x, T, log = one(sc.S, sc.y)
+                logs.append(log)
+            ctx.event(1)
+            if args.profile_region:
+                ctx.synchronize()
+                torch.cuda.profiler.stop()
+            ms_total = ctx.elapsed_ms(0, 1)
+            launches = ctx.launches - l0
+            clocks = clk.stop()
+            barrier(world)
+        finally:
+            ctx.set_precision("fp32")
+        ms = ms_total / args.steps
+        if world > 1:
+            ms = ranks_max(ms, "cuda:%d" % local)
+        ev = logs[-1].events
+        d = np.asarray(T, float) - np.asarray(sc.T_gt, float)
+        return {"ms": ms, "x": x, "one": one, "clocks": clocks, "launches": int(launches / args.steps),
+                "nrmse": nrmse(ctx, x, sc.x_gt_host),
+                "motion_max_err": {"trans_vox": float(np.max(np.abs(d[:, :3]))),
+                                   "rot_deg": float(np.degrees(np.max(np.abs(d[:, 3:]))))},
+                "schedule": {"outer": [sum(1 for e in ev if e["step"] == "lm" and e["level"] == lv) for lv in (0, 1)],
+                             "cg_final": sum(e["iters"] for e in ev if e["step"] == "cg" and e["level"] == 2)},
+                "proposals_kept": sum(e["accepted"] for e in ev if e["step"] == "proposal"),
+                "lm_state_steps": [sum(e["lm_states"] for e in ev if e["step"] == "lm" and e["level"] == lv)
+                                   for lv in (0, 1)],
+                "phases_s": {k: round(v, 4) for k, v in phase_split(logs[-1]).items()}}
+
+    # the plain method (FP32, no proposal): the NRMSE the headline must reach
+    plain = arm(False, "fp32")
+    err = plain["nrmse"]
+    # the headline: learned proposal + BF16x3 tensor-core DFT passes and Gram
+    head = plain if args.plain else arm(net is not None, head_prec)
+    ms = head["ms"]
+    one = head["one"]
+    counts = plain["schedule"]
 
     # end to end through the public API with host buffers (upload, recon, download)
     # inputs staged in pinned host memory (column-major, as the API expects)
@@ -780,26 +825,29 @@ def main():
 
     Sh, _Sbuf = pinned(sc.S)
     yh, _ybuf = pinned(sc.y)
-    # one untimed pass of the same path first (as the device-timed steps have
-    # warm-up steps): the device pool then holds the memory of the uploaded
-    # inputs instead of growing inside the timed region
-    Sd = ctx.upload(Sh)
-    yd = ctx.upload(yh)
-    xe, _, _ = one(Sd, yd)
-    xe.numpy()
-    del Sd, yd, xe
-    ctx.synchronize()
-    t0 = time.perf_counter()
-    eclk = NvmlClockSampler(local)
-    eclk.start()
-    ctx.event(2)
-    Sd = ctx.upload(Sh)
-    yd = ctx.upload(yh)
-    ctx.event(6)
-    xe, _, elog = one(Sd, yd)
-    ctx.event(7)
-    xh = xe.numpy()
-    ctx.event(3)
+    ctx.set_precision(head_prec)
+    try:
+        # one untimed pass of the same path first (as the device-timed steps have
+        # warm-up steps): the device pool then holds the memory of the uploaded
+        # inputs instead of growing inside the timed region
+        Sd = ctx.upload(Sh)
+        yd = ctx.upload(yh)
+        xe, _, _ = one(Sd, yd)
+        xe.numpy()
+        del Sd, yd, xe
+        ctx.synchronize()
+        eclk = NvmlClockSampler(local)
+        eclk.start()
+        ctx.event(2)
+        Sd = ctx.upload(Sh)
+        yd = ctx.upload(yh)
+        ctx.event(6)
+        xe, _, elog = one(Sd, yd)
+        ctx.event(7)
+        xh = xe.numpy()
+        ctx.event(3)
+    finally:
+        ctx.set_precision("fp32")
     e2e_ms = ctx.elapsed_ms(2, 3)
     e2e_parts = {"upload_s": ctx.elapsed_ms(2, 6) * 1e-3, "recon_s": ctx.elapsed_ms(6, 7) * 1e-3,
                  "download_s": ctx.elapsed_ms(7, 3) * 1e-3}
@@ -807,32 +855,39 @@ def main():
     e2e_clocks = eclk.stop()
     del Sd, yd, xh
 
-    # the same reconstruction with the learned motion proposal at the coarsest
-    # level (trained weights shipped with the package)
-    # the same reconstruction with the learned motion proposal, with the
-    # tensor-core DFT passes and Gram (BF16x3), and with both
+    # the two halves of the headline on their own: the learned proposal in
+    # FP32, and the tensor-core passes without the proposal (one run each)
     variants = {}
-    if not args.no_learned:
-        for name, lrn, prec in (("learned", True, "fp32"), ("mixed", False, "bf16x3"),
-                                ("learned_mixed", True, "bf16x3")):
-            variants[name] = variant_arm(ctx, sc, cfg, ms * 1e-3, err, learned=lrn, precision=prec)
+    if not args.no_learned and not args.plain:
+        for name, lrn, prec in (("learned", True, "fp32"), ("mixed", False, "bf16x3")):
+            variants[name] = variant_arm(ctx, sc, cfg, plain["ms"] * 1e-3, err, learned=lrn, precision=prec)
 
     # roofline of the north star's unit, the normal operator (encodedecode) at
     # full size, on its algorithmic bytes; the transform's line passes beside it
     peak, pkind = peaks()
     roof = normal_operator_roofline(ctx, cfg, peak, pkind)
+    roof_m = normal_operator_roofline(ctx, cfg, peak, pkind, precision="bf16x3")
     roof_t = transform_roofline(ctx, cfg, sc, peak, pkind)
 
+    if not args.plain:
+        config["workload"] = config["workload"].replace(
+            "plain FP32", "learned motion proposal + BF16x3 tensor-core DFT passes and coil Gram")
     out = {"metric": METRIC, "value": ms * 1e-3 / world, "unit": "s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-           "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic", "config": config,
-           "nrmse": err, "motion_max_err": {"trans_vox": motion_err[0], "rot_deg": motion_err[1]},
-           "schedule": counts, "phases_s": {k: round(v, 4) for k, v in phases.items()},
-           "gpu_launches": int(launches / args.steps), "clocks": clocks,
+           "vs_baseline": None, "dtype": "c64 (fp32 storage; %s products)" % head_prec, "data": "synthetic",
+           "config": config, "nrmse": head["nrmse"], "reaches_plain_nrmse": bool(head["nrmse"] <= 1.01 * err),
+           "motion_max_err": head["motion_max_err"], "schedule": head["schedule"],
+           "proposals_kept": head["proposals_kept"], "lm_state_steps": head["lm_state_steps"],
+           "phases_s": head["phases_s"], "gpu_launches": head["launches"], "clocks": head["clocks"],
+           "plain": {"value": plain["ms"] * 1e-3 / world, "unit": "s", "nrmse": err,
+                     "motion_max_err": plain["motion_max_err"], "schedule": plain["schedule"],
+                     "lm_state_steps": plain["lm_state_steps"], "phases_s": plain["phases_s"],
+                     "gpu_launches": plain["launches"], "clocks": plain["clocks"]},
+           "vs_plain": ms / plain["ms"],
            "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": int(Sh.nbytes + yh.nbytes),
                    "d2h_bytes_per_step": int(np.prod(cfg["N"]) * 8), "parts": {k: round(v, 4) for k, v in e2e_parts.items()},
                    "phases_s": {k: round(v, 4) for k, v in e2e_phases.items()}, "clocks": e2e_clocks},
-           "roofline": roof, "roofline_transform": roof_t}
+           "roofline": roof, "roofline_mixed": roof_m, "roofline_transform": roof_t}
     out.update(variants)
     if rank == 0 and not args.no_batch:
         # free the benchmark scan first: the batch holds about 45 GB of scans

@@ -22,6 +22,7 @@ reference's MATLAB dimension order with column-major memory: volumes
 """
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -51,13 +52,26 @@ class Context:
             raise DisorderError(st, "cannot create a context on CUDA device %d" % device)
         self.h = h
         self.device = device
+        # plans, device arrays and networks of this context: they are released
+        # before the context itself, whatever order the garbage collector
+        # finalises a cycle that holds them in
+        self._children = weakref.WeakSet()
 
     def check(self, st):
         if st:
             raise DisorderError(st, self.lib.disorder_last_error(self.h).decode())
 
+    def adopt(self, obj):
+        """Register an object with a close() that must run before the context goes."""
+        self._children.add(obj)
+
     def close(self):
         if getattr(self, "h", None):
+            for ch in list(getattr(self, "_children", ())):
+                try:
+                    ch.close()
+                except Exception:
+                    pass
             self.lib.disorder_ctx_destroy(self.h)
             self.h = None
 
@@ -129,6 +143,7 @@ class DeviceArray:
         p = C.c_void_p()
         ctx.check(ctx.lib.disorder_malloc(ctx.h, max(self.nbytes, 1), C.byref(p)))
         self.ptr = p.value
+        ctx.adopt(self)
 
     def numpy(self):
         out = np.empty(self.shape, dtype=self.dtype, order="F")
@@ -140,6 +155,9 @@ class DeviceArray:
         if self.ptr is not None and self.ctx.h is not None:
             self.ctx.lib.disorder_free(self.ctx.h, self.ptr)
         self.ptr = None
+
+    def close(self):
+        self.free()
 
     def __del__(self):
         try:
@@ -252,12 +270,18 @@ class Plan:
         self.n_mot = sd.n_mot
         self.n_samples = int(off[-1])
         self.nEc = off.copy()
+        ctx.adopt(self)
+
+    def close(self):
+        # a plan goes before its context (disorder_plan_destroy uses the
+        # context's stream); once the context is gone there is nothing to free
+        if getattr(self, "h", None) is not None and self.ctx.h is not None:
+            self.ctx.lib.disorder_plan_destroy(self.h)
+        self.h = None
 
     def __del__(self):
         try:
-            if self.h is not None:
-                self.ctx.lib.disorder_plan_destroy(self.h)
-                self.h = None
+            self.close()
         except Exception:
             pass
 

@@ -69,6 +69,27 @@ int dis_small(disorder_ctx_s* ctx, Workspace* ws) {
   return DISORDER_OK;
 }
 
+int dis_ctas_per_sm(const void* fn, int threads, size_t dyn_smem) {
+  cudaFuncAttributes fa;
+  int dev = 0, smem_sm = 0, res_blk = 0, regs_sm = 0, thr_sm = 0, blk_sm = 0;
+  if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&res_blk, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&blk_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev) != cudaSuccess || threads <= 0) {
+    cudaGetLastError();
+    return 0;
+  }
+  const long long smem_blk = (long long)dyn_smem + (long long)fa.sharedSizeBytes + res_blk;
+  const int warps = (threads + 31) / 32;
+  const long long regs_blk = (long long)warps * 32 * ((fa.numRegs + 7) / 8 * 8);  // 8-register granules
+  long long n = std::min<long long>(thr_sm / threads, blk_sm);
+  if (smem_blk > 0) n = std::min<long long>(n, smem_sm / smem_blk);
+  if (regs_blk > 0) n = std::min<long long>(n, regs_sm / regs_blk);
+  return (int)std::max<long long>(n, 0);
+}
+
 static bool use_pool() {
   static const bool v = [] {
     const char* e = std::getenv("DISORDER_POOL");
@@ -419,6 +440,11 @@ int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* g, const di
     for (long long i = p->seg_off[s]; i < p->seg_off[s + 1]; ++i) perm[p->seg_off[s] + fill[smp->ky[i]]++] = (int)i;
     for (int k = 0; k <= N1; ++k) rp[k] += (int)p->seg_off[s];
   }
+  std::vector<int> kyq(ns), kzq(ns);
+  for (long long q = 0; q < ns; ++q) {
+    kyq[q] = smp->ky[perm[q]];
+    kzq[q] = smp->kz[perm[q]];
+  }
   auto up = [&](void** d, const void* h, size_t bytes) -> bool {
     if (cudaMalloc(d, std::max<size_t>(bytes, 4)) != cudaSuccess) return false;
     return !bytes || cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
@@ -426,6 +452,7 @@ int disorder_plan_create(disorder_ctx ctx, const disorder_grid_desc* g, const di
   if (!up((void**)&p->d_ky, smp->ky, sizeof(int) * ns) || !up((void**)&p->d_kz, smp->kz, sizeof(int) * ns) ||
       !up((void**)&p->d_seg_of, segof.data(), sizeof(int) * ns) ||
       !up((void**)&p->d_perm, perm.data(), sizeof(int) * ns) ||
+      !up((void**)&p->d_kyq, kyq.data(), sizeof(int) * ns) || !up((void**)&p->d_kzq, kzq.data(), sizeof(int) * ns) ||
       !up((void**)&p->d_rowptr, rowptr.data(), sizeof(int) * rowptr.size()) ||
       !up((void**)&p->d_seg_off, p->seg_off.data(), sizeof(long long) * p->seg_off.size()))
     return fail(dis_set_error(ctx, DISORDER_OOM, "plan: sample table allocation or upload: %s",
@@ -447,6 +474,8 @@ int disorder_plan_destroy(disorder_plan p) {
   cudaFree(p->d_kz);
   cudaFree(p->d_seg_of);
   cudaFree(p->d_perm);
+  cudaFree(p->d_kyq);
+  cudaFree(p->d_kzq);
   cudaFree(p->d_rowptr);
   cudaFree(p->d_seg_off);
   delete p;

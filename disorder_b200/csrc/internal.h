@@ -74,6 +74,8 @@ struct disorder_plan_s {
   // d_perm[d_rowptr[s*(N1+1)+ky] .. d_rowptr[s*(N1+1)+ky+1])
   int* d_rowptr = nullptr;
   int* d_perm = nullptr;
+  int* d_kyq = nullptr;     // ky, kz of the sample at each CSR position
+  int* d_kzq = nullptr;
   int* d_seg_of = nullptr;  // segment of each sample
   long long* d_seg_off = nullptr;
   float2* d_tw[3] = {nullptr, nullptr, nullptr};  // exp(-2 pi i m / N[axis]), m < N[axis]
@@ -225,3 +227,7 @@ int dis_gram_umma(disorder_ctx_s* ctx, const float2* S, int C, long long V, floa
 
 // launch accounting
 inline void dis_count(disorder_ctx_s* ctx, int n = 1) { ctx->launches += n; }
+
+// CTAs of a kernel that fit on one SM of the current device by its registers,
+// shared memory (with the largest carveout) and threads; 0 on error
+int dis_ctas_per_sm(const void* fn, int threads, size_t dyn_smem);

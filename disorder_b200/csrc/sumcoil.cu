@@ -17,8 +17,9 @@
 //     reduction adds the N2 / LPB tiles into y (times the DFT scale, minus the
 //     measured samples when given);
 //   adjoint: per coil the CTA rebuilds its LPB columns of X from the samples,
-//     one thread per ky row (each row's samples are contiguous in ky order,
-//     so no two threads write the same element), X[b, ky] = sum_{i in row ky}
+//     one thread per ky row and half of the lines (each row's samples are
+//     contiguous in ky order, so no two threads write the same element),
+//     X[b, ky] = sum_{i in row ky}
 //     w_i y_i conj(W2^{kz_i b}), inverse-FFTs along dim 1 and accumulates
 //     conj(S_c) .* (...) over the coils in registers; one store of u.
 // Per state this moves 8 V (z) + 8 V (u) + the coil maps (shared by the
@@ -45,8 +46,8 @@ struct SumArgs {
   const int* slot_seg;   // segment of each slot
   const int* rowptr;     // per-segment CSR over ky rows (global sample positions)
   const int* perm;       // sample index at each CSR position
-  const int* ky;
-  const int* kz;
+  const int* kyq;        // its ky and kz
+  const int* kzq;
   const float2* tw2;     // W_N2^m, m < N2
   float2* part;          // [slot][tile][c][n3][q]
   int ldp;               // q stride (most samples of a chunk segment)
@@ -73,9 +74,42 @@ DIS_D float2 pmul(float2 a, float2 b) {
 DIS_D float2 bc(float v) { return make_float2(v, v); }
 
 // Coils go two at a time: the pair's X values of one (b, ky) are one float4
-// (re of coil c, re of coil c+1, im of coil c, im of coil c+1), so a sample's
-// twiddles, its sample indices and one 16-byte load serve both coils and the
-// complex products are packed f32x2 operations across the pair.
+// (re, im of coil c, re, im of coil c+1), so a sample's twiddles, its sample
+// row and one 16-byte load serve both coils, and the complex products are
+// packed f32x2 operations across the pair. The twiddles W2^m sit in shared
+// memory; the samples' rows and columns come in CSR order (kyq, kzq), two
+// samples per thread and pass so their load and product chains overlap.
+
+// per sample of the forward sum: (re, im) accumulators of the coil pair and
+// the twiddle W2^{kz b} as broadcast pairs, advanced by W2^{kz} per line
+struct SumAcc {
+  float2 ARp, ARn, AI;  // sum w.x XX, sum w.y XY, sum (w.x XY + w.y XX)
+  float2 WX, WY;        // (w.x, w.x), (w.y, w.y)
+  float2 SX, SY, SYn;   // step: (s.x, s.x), (s.y, s.y), (-s.y, -s.y)
+  int ky;
+};
+
+DIS_D void acc_init(SumAcc& A, int ky, int kz, int b0, int N2, const float2* tws) {
+  const float2 w = tws[(int)(((long long)kz * b0) % N2)], st = tws[kz];
+  A.ARp = A.ARn = A.AI = make_float2(0.f, 0.f);
+  A.WX = bc(w.x);
+  A.WY = bc(w.y);
+  A.SX = bc(st.x);
+  A.SY = bc(st.y);
+  A.SYn = bc(-st.y);
+  A.ky = ky;
+}
+
+DIS_D void acc_line(SumAcc& A, const float4 x) {
+  const float2 XX = make_float2(x.x, x.z), XY = make_float2(x.y, x.w);
+  A.ARp = pfma(A.WX, XX, A.ARp);
+  A.ARn = pfma(A.WY, XY, A.ARn);
+  A.AI = pfma(A.WX, XY, A.AI);
+  A.AI = pfma(A.WY, XX, A.AI);
+  const float2 nx = pfma(A.WX, A.SX, pmul(A.WY, A.SYn));
+  A.WY = pfma(A.WX, A.SY, pmul(A.WY, A.SX));
+  A.WX = nx;
+}
 
 // forward: partial sample sums of one (slot, tile of LPB lines along b, n3)
 template <int F1, int F2>
@@ -84,12 +118,14 @@ __global__ void __launch_bounds__(kThreads) sum_fwd_kernel(SumArgs a, const floa
   using LN = ff::Line<F1, F2>;
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
   extern __shared__ __align__(16) float2 sm[];
-  float2* tw = sm;
+  float4* Xs = reinterpret_cast<float4*>(sm);  // [LPB][N] coil pairs
+  float2* Xh = sm;                             // the same, as (coil, re/im) halves
+  float2* tw = sm + 2 * LPB * N;
   float2* ex = tw + LN::TWS;
-  float4* Xs = reinterpret_cast<float4*>(ex + LPB * LN::EXSZ);  // [LPB][N] coil pairs
-  float* Xf = reinterpret_cast<float*>(Xs);
+  float2* tws = ex + LPB * LN::EXSZ;  // W2^m, m < N2
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
   ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
+  for (int m = tid; m < a.N2; m += kThreads) tws[m] = a.tw2[m];
   const int slot = (int)(blockIdx.x % a.n_slots);
   const long long q0 = (long long)(blockIdx.x / a.n_slots) * LPB;  // first line (b + N2 n3)
   const int n3 = (int)(q0 / a.N2), b0 = (int)(q0 % a.N2), tile = b0 / LPB;
@@ -116,35 +152,32 @@ __global__ void __launch_bounds__(kThreads) sum_fwd_kernel(SumArgs a, const floa
       LN::fwd(v, X, lt, myex, tw);
       if (lt < F1) {
 #pragma unroll
-        for (int k2 = 0; k2 < F2; ++k2) {
-          float* e = Xf + 4 * ((long long)li * N + lt + F1 * k2);
-          e[h] = X[k2].x;
-          e[2 + h] = X[k2].y;
-        }
+        for (int k2 = 0; k2 < F2; ++k2) Xh[2 * ((long long)li * N + lt + F1 * k2) + h] = X[k2];
       }
       __syncwarp();  // the line's exchange area is reused by the next FFT
     }
     __syncthreads();
     float2* out0 = a.part + ((((long long)slot * a.ntile + tile) * a.C + c) * a.N3c + n3) * a.ldp;
     float2* out1 = out0 + (long long)a.N3c * a.ldp;
-    for (int q = s0 + tid; q < s1; q += kThreads) {
-      const int i = a.perm[q];
-      const int ky = a.ky[i], kz = a.kz[i];
-      float2 w = a.tw2[(int)(((long long)kz * b0) % a.N2)];
-      const float2 st = a.tw2[kz];
-      float2 AR = make_float2(0.f, 0.f), AI = make_float2(0.f, 0.f);  // lanes: the two coils
+    for (int q = s0 + tid; q < s1; q += 2 * kThreads) {
+      const int qb = q + kThreads;
+      const bool hb = qb < s1;
+      SumAcc A, B;
+      acc_init(A, a.kyq[q], a.kzq[q], b0, a.N2, tws);
+      acc_init(B, hb ? a.kyq[qb] : A.ky, hb ? a.kzq[qb] : 0, b0, a.N2, tws);
 #pragma unroll
       for (int j = 0; j < LPB; ++j) {
-        const float4 x = Xs[j * N + ky];
-        const float2 XX = make_float2(x.x, x.y), XY = make_float2(x.z, x.w);
-        AR = pfma(bc(w.x), XX, AR);
-        AR = pfma(bc(-w.y), XY, AR);
-        AI = pfma(bc(w.x), XY, AI);
-        AI = pfma(bc(w.y), XX, AI);
-        w = cmul(w, st);
+        acc_line(A, Xs[j * N + A.ky]);
+        acc_line(B, Xs[j * N + B.ky]);
       }
-      out0[q - s0] = make_float2(AR.x, AI.x);
-      if (two) out1[q - s0] = make_float2(AR.y, AI.y);
+      const float2 RA = make_float2(A.ARp.x - A.ARn.x, A.ARp.y - A.ARn.y);
+      out0[q - s0] = make_float2(RA.x, A.AI.x);
+      if (two) out1[q - s0] = make_float2(RA.y, A.AI.y);
+      if (hb) {
+        const float2 RB = make_float2(B.ARp.x - B.ARn.x, B.ARp.y - B.ARn.y);
+        out0[qb - s0] = make_float2(RB.x, B.AI.x);
+        if (two) out1[qb - s0] = make_float2(RB.y, B.AI.y);
+      }
     }
     __syncthreads();  // Xs is rewritten by the next coil pair
   }
@@ -179,19 +212,21 @@ __global__ void sum_reduce_kernel(SumArgs a, float2* __restrict__ y, const float
 // adjoint: u[slot] (LPB lines) = scale * sum_c conj(S_c) .* IFFT_1(X_c), X_c
 // built from the weighted samples of the slot's segment
 template <int F1, int F2>
-__global__ void __launch_bounds__(kThreads) sum_adj_kernel(SumArgs a, const float2* __restrict__ y, long long ld,
+__global__ void __launch_bounds__(kThreads, 2) sum_adj_kernel(SumArgs a, const float2* __restrict__ y, long long ld,
                                                            int n3off, int N3y, const float* __restrict__ We,
                                                            const float* __restrict__ Mb, float2* __restrict__ u,
                                                            float scale, const float2* __restrict__ twg) {
   using LN = ff::Line<F1, F2>;
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
   extern __shared__ __align__(16) float2 sm[];
-  float2* tw = sm;
+  float4* Xs = reinterpret_cast<float4*>(sm);  // [LPB][N] coil pairs
+  const float2* Xh = sm;                       // the same, as (coil, re/im) halves
+  float2* tw = sm + 2 * LPB * N;
   float2* ex = tw + LN::TWS;
-  float4* Xs = reinterpret_cast<float4*>(ex + LPB * LN::EXSZ);  // [LPB][N] coil pairs
-  const float* Xf = reinterpret_cast<const float*>(Xs);
+  float2* tws = ex + LPB * LN::EXSZ;  // conj(W2^m), m < N2
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
   ff::load_tw<F1, F2>(tw, twg, tid, kThreads);
+  for (int m = tid; m < a.N2; m += kThreads) tws[m] = cconj(a.tw2[m]);
   const int slot = (int)(blockIdx.x % a.n_slots);
   const long long q0 = (long long)(blockIdx.x / a.n_slots) * LPB;
   const int n3 = (int)(q0 / a.N2), b0 = (int)(q0 % a.N2);
@@ -208,30 +243,45 @@ __global__ void __launch_bounds__(kThreads) sum_adj_kernel(SumArgs a, const floa
     const bool two = c + 1 < a.C;
     const long long yo0 = ld * (n3 + n3off) + ld * N3y * c;
     const long long yo1 = yo0 + ld * N3y;
-    for (int r = tid; r < a.N1; r += kThreads) {
-      float2 XR[LPB], XI[LPB];  // lanes: the two coils
+    // each row's LPB lines in two halves (rows first, so a warp's stores are
+    // consecutive): a thread sums the row's samples into LPB / 2 lines
+    constexpr int HL = LPB / 2;
+    for (int rr = tid; rr < 2 * a.N1; rr += kThreads) {
+      const int r = rr % a.N1, jb = (rr / a.N1) * HL;
+      float2 XR[HL], XI[HL];  // lanes: the two coils
 #pragma unroll
-      for (int j = 0; j < LPB; ++j) XR[j] = XI[j] = make_float2(0.f, 0.f);
-      for (int q = rp[r]; q < rp[r + 1]; ++q) {
-        const int i = a.perm[q];
-        const int kz = a.kz[i];
-        const float wt = We ? mb * We[i] : mb;
-        const float2 w = cconj(a.tw2[(int)(((long long)kz * b0) % a.N2)]);
-        const float2 st = cconj(a.tw2[kz]);
-        const float2 v0 = cmul(cscale(y[yo0 + i], wt), w);
-        const float2 v1 = two ? cmul(cscale(y[yo1 + i], wt), w) : make_float2(0.f, 0.f);
-        float2 VX = make_float2(v0.x, v1.x), VY = make_float2(v0.y, v1.y);
+      for (int j = 0; j < HL; ++j) XR[j] = XI[j] = make_float2(0.f, 0.f);
+      const int qe = rp[r + 1];
+      for (int q = rp[r]; q < qe; q += 2) {
+        // two samples of the row at a time; a missing second one adds zeros
+        const bool hb = q + 1 < qe;
+        const int i0 = a.perm[q], i1 = hb ? a.perm[q + 1] : i0;
+        const int kz0 = a.kzq[q], kz1 = hb ? a.kzq[q + 1] : kz0;
+        const float wt0 = We ? mb * We[i0] : mb, wt1 = hb ? (We ? mb * We[i1] : mb) : 0.f;
+        const float2 w0 = tws[(int)(((long long)kz0 * (b0 + jb)) % a.N2)], st0 = tws[kz0];
+        const float2 w1 = tws[(int)(((long long)kz1 * (b0 + jb)) % a.N2)], st1 = tws[kz1];
+        const float2 p0 = cmul(cscale(y[yo0 + i0], wt0), w0);
+        const float2 p1 = two ? cmul(cscale(y[yo1 + i0], wt0), w0) : make_float2(0.f, 0.f);
+        const float2 r0 = cmul(cscale(y[yo0 + i1], wt1), w1);
+        const float2 r1 = two ? cmul(cscale(y[yo1 + i1], wt1), w1) : make_float2(0.f, 0.f);
+        float2 VX = make_float2(p0.x, p1.x), VY = make_float2(p0.y, p1.y);
+        float2 UX = make_float2(r0.x, r1.x), UY = make_float2(r0.y, r1.y);
+        const float2 SX0 = bc(st0.x), SY0 = bc(st0.y), SN0 = bc(-st0.y);
+        const float2 SX1 = bc(st1.x), SY1 = bc(st1.y), SN1 = bc(-st1.y);
 #pragma unroll
-        for (int j = 0; j < LPB; ++j) {
-          XR[j] = cadd(XR[j], VX);
-          XI[j] = cadd(XI[j], VY);
-          const float2 nx = pfma(VX, bc(st.x), pmul(VY, bc(-st.y)));
-          VY = pfma(VX, bc(st.y), pmul(VY, bc(st.x)));
+        for (int j = 0; j < HL; ++j) {
+          XR[j] = cadd(XR[j], cadd(VX, UX));
+          XI[j] = cadd(XI[j], cadd(VY, UY));
+          const float2 nx = pfma(VX, SX0, pmul(VY, SN0));
+          VY = pfma(VX, SY0, pmul(VY, SX0));
           VX = nx;
+          const float2 ux = pfma(UX, SX1, pmul(UY, SN1));
+          UY = pfma(UX, SY1, pmul(UY, SX1));
+          UX = ux;
         }
       }
 #pragma unroll
-      for (int j = 0; j < LPB; ++j) Xs[j * N + r] = make_float4(XR[j].x, XR[j].y, XI[j].x, XI[j].y);
+      for (int j = 0; j < HL; ++j) Xs[(jb + j) * N + r] = make_float4(XR[j].x, XI[j].x, XR[j].y, XI[j].y);
     }
     __syncthreads();
 #pragma unroll
@@ -239,10 +289,8 @@ __global__ void __launch_bounds__(kThreads) sum_adj_kernel(SumArgs a, const floa
       if (h == 1 && !two) break;
       float2 X[F2], v[F1];
 #pragma unroll
-      for (int k2 = 0; k2 < F2; ++k2) {
-        const float* e = Xf + 4 * ((long long)li * N + lt + F1 * k2);
-        X[k2] = lt < F1 ? make_float2(e[h], e[2 + h]) : make_float2(0.f, 0.f);
-      }
+      for (int k2 = 0; k2 < F2; ++k2)
+        X[k2] = lt < F1 ? Xh[2 * ((long long)li * N + lt + F1 * k2) + h] : make_float2(0.f, 0.f);
       LN::inv(X, v, lt, myex, tw);
       __syncwarp();
       if (lt < F2) {
@@ -264,7 +312,10 @@ template <int F1, int F2>
 struct SumLaunch {
   using LN = ff::Line<F1, F2>;
   static constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
-  static size_t smem() { return sizeof(float2) * (LN::TWS + (size_t)LPB * LN::EXSZ) + sizeof(float4) * LPB * N; }
+  static constexpr int kMaxN2 = 512;  // the shared twiddle table W2^m
+  static size_t smem() {
+    return sizeof(float2) * (LN::TWS + (size_t)LPB * LN::EXSZ + kMaxN2) + sizeof(float4) * LPB * N;
+  }
   static bool init() {
     const int b = (int)smem();
     const int co = (int)cudaSharedmemCarveoutMaxShared;  // two CTAs per SM
@@ -327,7 +378,8 @@ bool dispatch(int n1, Fn&& f) {
 bool dis_sum_coil_usable(const disorder_plan_s* plan) {
   if (!plan->ctx || !plan->ctx->tune_coil || !dis_use_fast()) return false;
   const int lpb = sc::lines_per_cta(plan->N[0]);
-  return lpb > 0 && plan->N[1] % lpb == 0 && plan->N[0] <= 4 * fp::kThreads;
+  return lpb > 0 && plan->N[1] % lpb == 0 && plan->N[0] <= 4 * fp::kThreads &&
+         plan->N[1] <= sc::SumLaunch<16, 16>::kMaxN2;
 }
 
 // bytes of partial sums per slot for C coils, N3c readout rows and ldp samples
@@ -349,8 +401,8 @@ static sc::SumArgs sum_args(const disorder_plan_s* plan, const CoilArgs& a, floa
   s.slot_seg = a.d_slot_seg;
   s.rowptr = plan->d_rowptr;
   s.perm = plan->d_perm;
-  s.ky = plan->d_ky;
-  s.kz = plan->d_kz;
+  s.kyq = plan->d_kyq;
+  s.kzq = plan->d_kzq;
   s.tw2 = plan->d_tw[1];
   s.part = part;
   s.ldp = ldp;

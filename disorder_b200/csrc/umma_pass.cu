@@ -27,13 +27,22 @@
 // transposing steps (stage 1 -> 2 and 3 -> 4), where a thread scatters its
 // row's 16 values into 16 rows, hit 32 distinct banks per warp.
 //
+// Stages 3 and 4 use the conjugate DFT matrices; they run as the forward
+// matrices of stages 2 and 1 on conjugated operands (conj(W^-1 v) =
+// W conj(v)), so one 32 x 32 block serves all four stages when F2 = 16 and
+// two blocks (W_16, W_F2) when F2 = 11.
+//
 // Threads: 256; thread (warp w, lane i) owns accumulator row
 // 128 (w >> 2) + 32 (w & 3) + i, i.e. line l = (i & 7) + 8 (w & 1) and index
 // u = (i >> 3) + 8 (w >> 2) + 4 ((w >> 1) & 1), reading tensor-memory lanes of
-// its warp's quadrant. Tiles move by TMA exactly as in tmapass.cuh (no
-// cluster multicast, this GPU's buffers only), double buffered; every wait is
-// bounded and a wait that runs out sets the error word, drains the copies in
-// flight, frees the tensor memory and stops the CTA.
+// its warp's quadrant. Tiles move by TMA as in tmapass.cuh (no cluster
+// multicast, this GPU's buffers only) through one stage buffer: the next
+// tile's load is issued as soon as stage 1 has read the current one, and the
+// result is staged for its TMA store in the operand area, free after stage 4.
+// That keeps a CTA at 72 KB (BF16x3) or 107 KB (3xTF32) of shared memory,
+// three or two CTAs per SM, whose stages overlap one another's waits. Every
+// wait is bounded and a wait that runs out sets the error word, drains the
+// copies in flight, frees the tensor memory and stops the CTA.
 #include <cuda_bf16.h>
 
 #include "tmapass.cuh"
@@ -57,9 +66,11 @@ struct UCfg {
   static constexpr int BBYTES = 32 * 32 * ES;            // one part of one B
   static constexpr int TILE = 16 * N;                    // float2 per tile
   static constexpr int SBB = ((8 * TILE) + 1023) & ~1023;
-  // distinct DFT blocks: stages 1 and 2 (and 3 and 4) share theirs when F2 = 16
-  static constexpr int NBM = F2 == 16 ? 2 : 4;
-  static constexpr size_t SMEM = 1024 + 2 * (size_t)SBB + 2 * ABYTES + 2 * NBM * BBYTES + 8 * 16 * F2;
+  // distinct DFT blocks: W_16 (stages 1, 4) and W_F2 (stages 2, 3), one when F2 = 16
+  static constexpr int NBM = F2 == 16 ? 1 : 2;
+  static constexpr size_t SMEM = 1024 + (size_t)SBB + 2 * ABYTES + 2 * NBM * BBYTES + 8 * 16 * F2;
+  static constexpr int MIN_CTAS = TF32 ? 2 : 3;
+  static_assert(8 * TILE <= 2 * ABYTES, "the result tile is staged in the operand area");
 };
 
 DIS_D int rho(int l, int u) { return 32 * ((l >> 3) + 2 * (u >> 2)) + (l & 7) + 8 * (u & 3); }
@@ -131,21 +142,21 @@ DIS_D void row_load(uint32_t taddr, float2 (&v)[16]) {
 }
 
 template <int F2, bool TF32>
-__global__ void __launch_bounds__(kUT, 1)
+__global__ void __launch_bounds__(kUT, (UCfg<F2, TF32>::MIN_CTAS))
     umma_line_kernel(const __grid_constant__ CUtensorMap in_map, const __grid_constant__ CUtensorMap out_map,
                      TArgs t, const float2* __restrict__ twg, int n_tiles, int shared_input) {
   using U = UCfg<F2, TF32>;
   constexpr int N = U::N;
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ uint64_t tbar[2];
+  __shared__ uint64_t tbar;
   __shared__ uint64_t mbar;
   __shared__ uint32_t tbase;
   const uint32_t base_s = um::saddr(smraw);
   unsigned char* al = smraw + (((base_s + 1023u) & ~1023u) - base_s);
-  float2* stg0 = reinterpret_cast<float2*>(al);
-  float2* stg1 = reinterpret_cast<float2*>(al + U::SBB);
-  unsigned char* Ahi = al + 2 * U::SBB;
+  float2* st = reinterpret_cast<float2*>(al);
+  unsigned char* Ahi = al + U::SBB;
   unsigned char* Alo = Ahi + U::ABYTES;
+  float2* res = reinterpret_cast<float2*>(Ahi);  // the result tile, after stage 4
   unsigned char* Bm = Alo + U::ABYTES;  // [block][part] blocks of BBYTES
   float2* tws = reinterpret_cast<float2*>(Bm + 2 * U::NBM * U::BBYTES);  // [t][k1] = W_N^{t k1}
   const int tid = threadIdx.x, w = tid >> 5, i = tid & 31;
@@ -153,16 +164,13 @@ __global__ void __launch_bounds__(kUT, 1)
   const int mu = (i >> 3) + 8 * (w >> 2) + 4 * ((w >> 1) & 1);  // this thread's index (t or k1)
   const int myrow = rho(ml, mu);
 
-  // ---- constant operands: the 32 x 32 real DFT blocks of the stages, and twiddles
+  // ---- constant operands: the 32 x 32 real DFT blocks, and twiddles
   for (int e = tid; e < U::NBM * 32 * 32; e += kUT) {
     const int blk = e / 1024, n = (e / 32) % 32, k = e % 32;
-    const int s = F2 == 16 ? 2 * blk : blk;  // the stage whose matrix block blk holds
     const int jo = n >> 1, ro = n & 1, ji = k >> 1, ri = k & 1;
     float2 W = make_float2(0.f, 0.f);
-    if (s == 0) W = twg[(F2 * ji * jo) % N];                                       // W_16^{m k1}, m = ji
-    if (s == 1 && jo < F2 && ji < F2) W = twg[(16 * ji * jo) % N];                 // W_F2^{t k2}, t = ji
-    if (s == 2 && jo < F2 && ji < F2) W = cconj(twg[(16 * ji * jo) % N]);          // W_F2^{-k2 t}, k2 = ji
-    if (s == 3) W = cconj(twg[(F2 * ji * jo) % N]);                                // W_16^{-k1 m}, k1 = ji
+    if (blk == 0) W = twg[(F2 * ji * jo) % N];                            // W_16^{m k1} (symmetric)
+    if (blk == 1 && jo < F2 && ji < F2) W = twg[(16 * ji * jo) % N];      // W_F2^{t k2} (symmetric)
     const float val = ro == 0 ? (ri == 0 ? W.x : -W.y) : (ri == 0 ? W.y : W.x);
     unsigned char* hb = Bm + (2 * blk) * U::BBYTES;
     unsigned char* lb = hb + U::BBYTES;
@@ -181,8 +189,7 @@ __global__ void __launch_bounds__(kUT, 1)
   }
   for (int e = tid; e < 16 * F2; e += kUT) tws[e] = twg[((e / 16) * (e % 16)) % N];
   if (tid == 0) {
-    um::bar_init(&tbar[0], 1);
-    um::bar_init(&tbar[1], 1);
+    um::bar_init(&tbar, 1);
     um::bar_init(&mbar, 1);
     fp::fence_async_smem();
   }
@@ -212,23 +219,27 @@ __global__ void __launch_bounds__(kUT, 1)
     it.ca = (tile - it.cb * nt0) * 16;
     it.nv = min(16, t.Nv[0] - it.ca);
   };
-  auto issue = [&](const PItem& it, float2* st, uint64_t* bar) {
+  auto issue = [&](const PItem& it) {
     if (t.skip_loads) return;
-    fp::mbar_expect_tx(bar, 8u * U::TILE);
+    fp::mbar_expect_tx(&tbar, 8u * U::TILE);
     fp::tma_load_tile(st, &in_map, it.ca, t.axis == 2 ? it.cb : 0, t.axis == 1 ? it.cb : 0,
-                      shared_input ? 0 : it.slot, bar);
+                      shared_input ? 0 : it.slot, &tbar);
   };
   uint32_t mph = 0;
   bool failed = false;
-  // one stage: the MMAs of all products, then a bounded wait for them
-  auto stage = [&](int s) -> bool {
+  PItem cur, nxt;
+  bool has_next = false;
+  int inflight = -1;  // item whose tile load is issued and not yet waited for
+  // one stage: the MMAs of all products, then a bounded wait for them; stage
+  // 0 also issues the next tile's load (its operand has read the buffer)
+  auto stage = [&](int s, int j) -> bool {
     um::fence_smem_async();
     um::fence_before_sync();
     __syncthreads();
     if (tid == 0) {
       um::fence_after_sync();
       const uint32_t a0 = um::saddr(Ahi), a1 = um::saddr(Alo);
-      const int blk = F2 == 16 ? (s >> 1) : s;
+      const int blk = F2 == 16 ? 0 : ((s == 0 || s == 3) ? 0 : 1);
       const uint32_t b0 = um::saddr(Bm + (2 * blk) * U::BBYTES), b1 = b0 + U::BBYTES;
       const uint32_t lboA = 256 * 16, lboB = 32 * 16;
 #pragma unroll
@@ -251,7 +262,12 @@ __global__ void __launch_bounds__(kUT, 1)
         }
       }
       um::commit(&mbar);
+      if (s == 0 && has_next) {
+        fp::fence_async_smem();
+        issue(nxt);
+      }
     }
+    if (s == 0 && has_next) inflight = j + 1;
     const bool ok = um::bar_wait(&mbar, mph, kMmaWait);
     mph ^= 1;
     if (__syncthreads_or(!ok)) return false;
@@ -259,12 +275,10 @@ __global__ void __launch_bounds__(kUT, 1)
     return true;
   };
 
-  PItem cur;
-  int inflight = -1;  // stage buffer of a tile load issued and not yet waited for
   if (n_items > 0) unit(b / S, b % S, cur);
-  if (n_items > 0 && tid == 0) issue(cur, stg0, &tbar[0]);
+  if (n_items > 0 && tid == 0) issue(cur);
+  if (n_items > 0) inflight = 0;
   for (int j = 0; j < n_items && !failed; ++j) {
-    float2* st = (j & 1) ? stg1 : stg0;
     // seeds of this thread's line (row (line, k1) of stage 2)
     float2 slo, shi, sst;
     {
@@ -276,9 +290,10 @@ __global__ void __launch_bounds__(kUT, 1)
       sst = sr[32];
     }
     bool late = false;
+    if (tid == 0) fp::bulk_wait_read0();  // the previous result's store has read the operand area
     {
       uint32_t spins = 0;
-      while (!fp::mbar_try_wait(&tbar[j & 1], (uint32_t)((j >> 1) & 1)))
+      while (!fp::mbar_try_wait(&tbar, (uint32_t)(j & 1)))
         if (++spins > t.wait_limit) {
           late = true;
           break;
@@ -289,20 +304,14 @@ __global__ void __launch_bounds__(kUT, 1)
       break;
     }
     inflight = -1;
-    PItem nxt = cur;
-    if (j + 1 < n_items) {
+    has_next = j + 1 < n_items;
+    if (has_next) {
       int slot = cur.slot + gr, tile = cur.tile + gq;
       if (slot >= S) {
         slot -= S;
         ++tile;
       }
       unit(tile, slot, nxt);
-      if (tid == 0) {
-        fp::bulk_wait_read0();  // item j-1's store has read the other buffer
-        fp::fence_async_smem();
-        issue(nxt, (j & 1) ? stg0 : stg1, &tbar[(j + 1) & 1]);
-      }
-      inflight = j + 1;
     }
     float2 v[16];
     // stage 1 operand: own row (line, t), K = m
@@ -312,7 +321,7 @@ __global__ void __launch_bounds__(kUT, 1)
       for (int m = 0; m < 16; ++m) v[m] = tt < F2 ? st[fp::tswz(tt + F2 * m, ml)] : make_float2(0.f, 0.f);
       put_row<TF32>(Ahi, Alo, myrow, v);
     }
-    if (!stage(0)) {
+    if (!stage(0, j)) {
       failed = true;
       break;
     }
@@ -326,11 +335,12 @@ __global__ void __launch_bounds__(kUT, 1)
         put_pair<TF32>(Ahi, Alo, rho(ml, k1), 256, tt, z);
       }
     }
-    if (!stage(1)) {
+    if (!stage(1, j)) {
       failed = true;
       break;
     }
-    // stage 2 -> 3: X[k1 + 16 k2] times the phase factor, own row, K = k2
+    // stage 2 -> 3: X[k1 + 16 k2] times the phase factor, conjugated (stage 3
+    // runs the forward W_F2 block), own row, K = k2
     row_load(trow, v);
     {
       constexpr int KP = F2 / 2;
@@ -351,38 +361,40 @@ __global__ void __launch_bounds__(kUT, 1)
           c = shi;
           if (k2 + 1 < F2) shi = cmul(shi, sst);
         }
-        v[k2] = cmul(c, v[k2]);
+        v[k2] = cconj(cmul(c, v[k2]));
       }
       put_row<TF32>(Ahi, Alo, myrow, v);
     }
-    if (!stage(2)) {
+    if (!stage(2, j)) {
       failed = true;
       break;
     }
-    // stage 3 -> 4: twiddle W_N^{-t k1}, scatter into rows (line, t), K = k1
+    // stage 3 -> 4: the accumulator holds conj(z); conj(z W_N^{-t k1}) =
+    // conj(z) W_N^{t k1}, scattered into rows (line, t), K = k1
     row_load(trow, v);
     {
       const int k1 = mu;
 #pragma unroll
       for (int tt = 0; tt < 16; ++tt) {
-        const float2 z = tt < F2 ? cmulc(v[tt], tws[tt * 16 + k1]) : make_float2(0.f, 0.f);
+        const float2 z = tt < F2 ? cmul(v[tt], tws[tt * 16 + k1]) : make_float2(0.f, 0.f);
         put_pair<TF32>(Ahi, Alo, rho(ml, tt), 256, k1, z);
       }
     }
-    if (!stage(3)) {
+    if (!stage(3, j)) {
       failed = true;
       break;
     }
-    // stage 4 result: row (line, t) holds y[t + F2 m]; back into the tile
+    // stage 4 result: row (line, t) holds conj(y[t + F2 m]); staged in the
+    // operand area (the MMAs that read it are complete) for the TMA store
     row_load(trow, v);
     if (mu < F2) {
 #pragma unroll
-      for (int m = 0; m < 16; ++m) st[fp::tswz(mu + F2 * m, ml)] = v[m];
+      for (int m = 0; m < 16; ++m) res[fp::tswz(mu + F2 * m, ml)] = cconj(v[m]);
     }
     fp::fence_async_smem();  // the writes above are read by the bulk store
     __syncthreads();
     if (tid == 0) {
-      fp::tma_store_tile(&out_map, cur.ca, t.axis == 2 ? cur.cb : 0, t.axis == 1 ? cur.cb : 0, cur.slot, st);
+      fp::tma_store_tile(&out_map, cur.ca, t.axis == 2 ? cur.cb : 0, t.axis == 1 ? cur.cb : 0, cur.slot, res);
       fp::bulk_commit();
     }
     cur = nxt;
@@ -391,8 +403,7 @@ __global__ void __launch_bounds__(kUT, 1)
     atomicExch(t.err, 1);
     // a tile load still in flight lands before the shared memory is released
     if (inflight >= 0 && !t.skip_loads)
-      for (uint32_t k = 0;
-           k < t.wait_limit && !fp::mbar_try_wait(&tbar[inflight & 1], (uint32_t)((inflight >> 1) & 1)); ++k) {
+      for (uint32_t k = 0; k < t.wait_limit && !fp::mbar_try_wait(&tbar, (uint32_t)(inflight & 1)); ++k) {
       }
   }
   if (tid == 0) fp::bulk_wait0();
@@ -419,9 +430,8 @@ bool launch_umma(const CUtensorMap& in, const CUtensorMap& out, const TArgs& t, 
   const long long units = tiles * t.n_vol;
   if (units == 0 || units >= (1LL << 31)) return false;
   static const int per_sm = [] {
-    int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, umma_line_kernel<F2, TF32>, kUT, U::SMEM);
-    return n < 1 ? 1 : (n > 2 ? 2 : n);  // at most 2 x 64 tensor-memory columns per SM
+    const int n = dis_ctas_per_sm(reinterpret_cast<const void*>(umma_line_kernel<F2, TF32>), kUT, U::SMEM);
+    return n < 1 ? 1 : (n > 4 ? 4 : n);  // at most 4 x 64 tensor-memory columns per SM
   }();
   const long long cap = (long long)sm_count * per_sm;
   const unsigned grid = (unsigned)(units < cap ? units : cap);

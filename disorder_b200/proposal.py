@@ -67,6 +67,7 @@ class MotionNet:
         Dv = (C.c_int32 * 3)(*self.D)
         ctx.check(ctx.lib.disorder_net_create(ctx.h, Dv, self.max_batch, C.byref(h)))
         self.h = h
+        ctx.adopt(self)
         self.P = param_count()
         self.step = 0
         self.set_params(init_params(np.random.default_rng(0)) if params is None else params)

@@ -47,6 +47,9 @@ typedef struct disorder_plan_s* disorder_plan;
 /* ---- context, stream and memory (replaces MATLAB gpuArray/gather,
  *      Methods/fftGPU.m:27-31 device selection; the MEX handle layer) ---- */
 int disorder_ctx_create(int device, disorder_ctx* out);
+/* Plans, networks and device memory of a context are released before it:
+ * disorder_plan_destroy, disorder_net_destroy and disorder_free use the
+ * context's stream. */
 int disorder_ctx_destroy(disorder_ctx ctx);
 const char* disorder_last_error(disorder_ctx ctx);
 int disorder_ctx_set_stream(disorder_ctx ctx, void* cuda_stream); /* NULL: own stream */
