@@ -174,6 +174,7 @@ int disorder_ctx_destroy(disorder_ctx ctx) {
   if (ctx->ws2) cudaFree(ctx->ws2);
   if (ctx->small) cudaFree(ctx->small);
   if (ctx->d_err) cudaFree(ctx->d_err);
+  if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);

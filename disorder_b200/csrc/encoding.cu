@@ -76,6 +76,7 @@ struct CoilPlan {
   bool sum = false;
   int ldp = 0;
   size_t per_slot = 0;  // coil-stage workspace bytes per slot
+  size_t gather = 0;    // sample-sum adjoint: its gathered samples per slot
 };
 static CoilPlan coil_plan(const disorder_plan_s* plan, int C, int N3c, const std::vector<int>& segs) {
   CoilPlan p;
@@ -87,6 +88,7 @@ static CoilPlan coil_plan(const disorder_plan_s* plan, int C, int N3c, const std
   p.sum = true;
   p.ldp = ldp;
   p.per_slot = pb;
+  p.gather = dis_sum_gather_bytes(C, N3c, ldp);
   return p;
 }
 
@@ -344,7 +346,7 @@ int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
     return DISORDER_OK;
   }
   const CoilPlan cp = coil_plan(plan, sp.C, N3, sp.segs);
-  const size_t coil = cp.sum ? 0 : cp.per_slot;  // the adjoint sample-sum stage needs no buffer
+  const size_t coil = cp.sum ? cp.gather : cp.per_slot;
   const int ch = chunk_for(plan, coil, V * sizeof(float2), nsg);
   const size_t need = (size_t)ch * (coil + V * sizeof(float2)) + dis_table_bytes(plan, ch, false) + 4096 * 4;
   Workspace ws;
@@ -355,13 +357,13 @@ int dis_decode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, const 
     std::vector<int> segs(sp.segs.begin() + c0, sp.segs.begin() + c0 + n);
     int* d_seg = nullptr;
     DIS_TRY(dis_upload_ints(ctx, &w, segs, &d_seg));
-    float2* A = cp.sum ? nullptr : w.take<float2>((size_t)n * sp.C * V);
+    float2* A = w.take<float2>((size_t)n * (cp.sum ? cp.gather / sizeof(float2) : (size_t)sp.C * V));
     float2* U = w.take<float2>((size_t)n * V);
-    if ((!cp.sum && !A) || !U) return dis_set_error(ctx, DISORDER_OOM, "decode: workspace too small");
+    if (!A || !U) return dis_set_error(ctx, DISORDER_OOM, "decode: workspace too small");
     CoilArgs ca = coil_args(plan, sp.Sf, sp.C, 0, N3, V, n, d_seg);
     const float scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
     if (cp.sum) {
-      DIS_TRY(dis_coil_sum_adj(ctx, plan, ca, sp.y, plan->n_samples, 0, N3, sp.We, sp.Mb, U, scale));
+      DIS_TRY(dis_coil_sum_adj(ctx, plan, ca, sp.y, plan->n_samples, 0, N3, sp.We, sp.Mb, U, scale, A, cp.ldp));
     } else {
       DIS_TRY(dis_coil_scatter_ifft2(ctx, plan, ca, sp.y, plan->n_samples, 0, N3, sp.We, sp.Mb, A));
       DIS_TRY(dis_coil_ifft1_combine(ctx, plan, ca, A, U, scale));
@@ -416,8 +418,8 @@ int dis_backproject_states(disorder_ctx_s* ctx, const disorder_plan_s* plan, con
   std::vector<int> all(S);
   for (int j = 0; j < S; ++j) all[j] = j;
   const CoilPlan cp = coil_plan(plan, C, N3, all);
-  const size_t coil = cp.sum ? 0 : cp.per_slot;
-  const int ch = cp.sum ? S : dis_chunk_slots(plan, C, N3, 0, S);
+  const size_t coil = cp.sum ? cp.gather : cp.per_slot;
+  const int ch = cp.sum ? chunk_for(plan, coil, 0, S) : dis_chunk_slots(plan, C, N3, 0, S);
   Workspace ws;
   DIS_TRY(dis_workspace(ctx, (size_t)ch * coil + dis_table_bytes(plan, ch, false) + 4096 * 4, &ws));
   const float scale = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
@@ -431,7 +433,9 @@ int dis_backproject_states(disorder_ctx_s* ctx, const disorder_plan_s* plan, con
     float2* U = out + (long long)c0 * V;
     CoilArgs ca = coil_args(plan, Sf, C, 0, N3, V, n, d_seg);
     if (cp.sum) {
-      DIS_TRY(dis_coil_sum_adj(ctx, plan, ca, r, plan->n_samples, 0, N3, nullptr, nullptr, U, scale));
+      float2* Q = w.take<float2>((size_t)n * cp.gather / sizeof(float2));
+      if (!Q) return dis_set_error(ctx, DISORDER_OOM, "back-projection: workspace too small");
+      DIS_TRY(dis_coil_sum_adj(ctx, plan, ca, r, plan->n_samples, 0, N3, nullptr, nullptr, U, scale, Q, cp.ldp));
     } else {
       float2* A = w.take<float2>((size_t)n * C * V);
       if (!A) return dis_set_error(ctx, DISORDER_OOM, "back-projection: workspace too small");
@@ -539,7 +543,8 @@ int dis_encodedecode_segments(disorder_ctx_s* ctx, const disorder_plan_s* plan, 
       const float s1 = (float)(1.0 / std::sqrt((double)plan->N[0] * plan->N[1]));
       DIS_TRY(dis_coil_sum_fwd(ctx, plan, ca, z, A, cp.ldp, ysb, plan->n_samples, 0, N3, nullptr, s1));
       ca.Vz = V;
-      DIS_TRY(dis_coil_sum_adj(ctx, plan, ca, ysb, plan->n_samples, 0, N3, sp.We, nullptr, U, s1));
+      // (the partial sums are reduced by now: their buffer takes the gathered samples)
+      DIS_TRY(dis_coil_sum_adj(ctx, plan, ca, ysb, plan->n_samples, 0, N3, sp.We, nullptr, U, s1, A, cp.ldp));
     } else {
       DIS_TRY(dis_coil_expand_fft1(ctx, plan, ca, z, A));
       DIS_TRY(dis_coil_fft2_weight(ctx, plan, ca, A, sp.wmap, sp.ys, plan->n_samples, 0, N3));

@@ -70,7 +70,9 @@ size_t dis_sum_part_bytes(const disorder_plan_s* plan, int C, int N3c, int ldp);
 int dis_coil_sum_fwd(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* z,
                      float2* part, int ldp, float2* y, long long y_ld, int y_n3off, int y_N3, const float2* y_meas,
                      float scale);
+size_t dis_sum_gather_bytes(int C, int N3c, int ldq);
 int dis_coil_sum_adj(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* y,
-                     long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* u, float scale);
+                     long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* u, float scale,
+                     float2* yq, int ldq);
 int dis_sum_slots(disorder_ctx_s* ctx, const float2* u, long long V, int n_slots, float2* out, float beta);
 int dis_broadcast(disorder_ctx_s* ctx, const float2* x, long long V, int n_slots, float2* out);

@@ -26,6 +26,9 @@ struct disorder_ctx_s {
   size_t small_bytes = 0;
   cudaEvent_t ev[16] = {};
   int* d_err = nullptr;  // device error word of bounded in-kernel waits (0: none)
+  // pinned host words the solvers' reductions land in (one set per context:
+  // contexts driven from different host threads must not share them)
+  void* h_scalars = nullptr;
   // the static scratch array of disorder_sinc_rigid_transform_static on this
   // device, resolved at context creation (null if that failed)
   void* static_scratch = nullptr;

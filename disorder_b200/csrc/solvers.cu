@@ -196,9 +196,8 @@ static int red_init(disorder_ctx_s* ctx, Workspace* ws, Reducer* R) {
   R->part = ws->take<d2>(kRedBlocks);
   R->res = ws->take<d2>(1);
   if (!R->part || !R->res) return dis_set_error(ctx, DISORDER_OOM, "reduction workspace");
-  static d2* pinned = nullptr;
-  if (!pinned) DIS_CUDA_TRY(cudaMallocHost(&pinned, sizeof(d2) * 4));
-  R->host = pinned;
+  if (!ctx->h_scalars) DIS_CUDA_TRY(cudaMallocHost(&ctx->h_scalars, sizeof(d2) * 4));
+  R->host = static_cast<d2*>(ctx->h_scalars);
   return DISORDER_OK;
 }
 

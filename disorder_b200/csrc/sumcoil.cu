@@ -49,7 +49,7 @@ struct SumArgs {
   const int* kyq;        // its ky and kz
   const int* kzq;
   const float2* tw2;     // W_N2^m, m < N2
-  float2* part;          // [slot][tile][c][n3][q]
+  float2* part;          // forward: [slot][tile][c][n3][q]; adjoint: the weighted samples [slot][c][n3][q]
   int ldp;               // q stride (most samples of a chunk segment)
   int ntile;             // N2 / LPB
 };
@@ -111,9 +111,11 @@ DIS_D void acc_line(SumAcc& A, const float4 x) {
   A.WX = nx;
 }
 
+constexpr int kG = 4;  // samples per thread and pass of the forward sum
+
 // forward: partial sample sums of one (slot, tile of LPB lines along b, n3)
 template <int F1, int F2>
-__global__ void __launch_bounds__(kThreads) sum_fwd_kernel(SumArgs a, const float2* __restrict__ z,
+__global__ void __launch_bounds__(kThreads, 2) sum_fwd_kernel(SumArgs a, const float2* __restrict__ z,
                                                            const float2* __restrict__ twg) {
   using LN = ff::Line<F1, F2>;
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
@@ -159,24 +161,32 @@ __global__ void __launch_bounds__(kThreads) sum_fwd_kernel(SumArgs a, const floa
     __syncthreads();
     float2* out0 = a.part + ((((long long)slot * a.ntile + tile) * a.C + c) * a.N3c + n3) * a.ldp;
     float2* out1 = out0 + (long long)a.N3c * a.ldp;
-    for (int q = s0 + tid; q < s1; q += 2 * kThreads) {
-      const int qb = q + kThreads;
-      const bool hb = qb < s1;
-      SumAcc A, B;
-      acc_init(A, a.kyq[q], a.kzq[q], b0, a.N2, tws);
-      acc_init(B, hb ? a.kyq[qb] : A.ky, hb ? a.kzq[qb] : 0, b0, a.N2, tws);
+    // four consecutive CSR positions per thread: most share a ky row, whose
+    // X values one shared-memory load per line serves
+    for (int qg = s0 + kG * tid; qg < s1; qg += kG * kThreads) {
+      SumAcc A[kG];
+#pragma unroll
+      for (int k = 0; k < kG; ++k) {
+        // positions past the segment repeat the previous row (no extra loads)
+        const bool in = qg + k < s1;
+        acc_init(A[k], in ? a.kyq[qg + k] : (k ? A[k - 1].ky : 0), in ? a.kzq[qg + k] : 0, b0, a.N2, tws);
+      }
 #pragma unroll
       for (int j = 0; j < LPB; ++j) {
-        acc_line(A, Xs[j * N + A.ky]);
-        acc_line(B, Xs[j * N + B.ky]);
+        float4 x = Xs[j * N + A[0].ky];
+        acc_line(A[0], x);
+#pragma unroll
+        for (int k = 1; k < kG; ++k) {
+          if (A[k].ky != A[k - 1].ky) x = Xs[j * N + A[k].ky];
+          acc_line(A[k], x);
+        }
       }
-      const float2 RA = make_float2(A.ARp.x - A.ARn.x, A.ARp.y - A.ARn.y);
-      out0[q - s0] = make_float2(RA.x, A.AI.x);
-      if (two) out1[q - s0] = make_float2(RA.y, A.AI.y);
-      if (hb) {
-        const float2 RB = make_float2(B.ARp.x - B.ARn.x, B.ARp.y - B.ARn.y);
-        out0[qb - s0] = make_float2(RB.x, B.AI.x);
-        if (two) out1[qb - s0] = make_float2(RB.y, B.AI.y);
+#pragma unroll
+      for (int k = 0; k < kG; ++k) {
+        if (qg + k >= s1) break;
+        const float2 R = make_float2(A[k].ARp.x - A[k].ARn.x, A[k].ARp.y - A[k].ARn.y);
+        out0[qg + k - s0] = make_float2(R.x, A[k].AI.x);
+        if (two) out1[qg + k - s0] = make_float2(R.y, A[k].AI.y);
       }
     }
     __syncthreads();  // Xs is rewritten by the next coil pair
@@ -209,13 +219,32 @@ __global__ void sum_reduce_kernel(SumArgs a, float2* __restrict__ y, const float
   }
 }
 
+// the adjoint's input: part[slot][c][n3][q - s0] = Mb[n3] We[i] y[i, n3, c]
+// for the sample i at CSR position q of the slot's segment (s0 its first)
+__global__ void sum_gather_kernel(SumArgs a, const float2* __restrict__ y, long long ld, int n3off, int N3y,
+                                  const float* __restrict__ We, const float* __restrict__ Mb) {
+  const long long per_slot = (long long)a.C * a.N3c * a.ldp;
+  const long long tot = per_slot * a.n_slots;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+    const int slot = (int)(e / per_slot);
+    const long long r = e % per_slot;  // (c, n3, k)
+    const int k = (int)(r % a.ldp);
+    const long long cn = r / a.ldp;
+    const int n3 = (int)(cn % a.N3c), c = (int)(cn / a.N3c);
+    const int* rp = a.rowptr + (long long)a.slot_seg[slot] * (a.N1 + 1);
+    if (k >= rp[a.N1] - rp[0]) continue;
+    const int i = a.perm[rp[0] + k];
+    float wt = Mb ? Mb[n3 + n3off] : 1.f;
+    if (We) wt *= We[i];
+    a.part[e] = cscale(y[i + ld * (n3 + n3off) + ld * N3y * c], wt);
+  }
+}
+
 // adjoint: u[slot] (LPB lines) = scale * sum_c conj(S_c) .* IFFT_1(X_c), X_c
-// built from the weighted samples of the slot's segment
+// built from the slot's gathered, weighted samples (sum_gather_kernel)
 template <int F1, int F2>
-__global__ void __launch_bounds__(kThreads, 2) sum_adj_kernel(SumArgs a, const float2* __restrict__ y, long long ld,
-                                                           int n3off, int N3y, const float* __restrict__ We,
-                                                           const float* __restrict__ Mb, float2* __restrict__ u,
-                                                           float scale, const float2* __restrict__ twg) {
+__global__ void __launch_bounds__(kThreads, 2) sum_adj_kernel(SumArgs a, float2* __restrict__ u, float scale,
+                                                              const float2* __restrict__ twg) {
   using LN = ff::Line<F1, F2>;
   constexpr int N = LN::N, TL = LN::TL, LPB = kThreads / TL;
   extern __shared__ __align__(16) float2 sm[];
@@ -234,15 +263,15 @@ __global__ void __launch_bounds__(kThreads, 2) sum_adj_kernel(SumArgs a, const f
   float2* myex = ex + li * LN::EXSZ;
   const int seg = a.slot_seg[slot];
   const int* rp = a.rowptr + (long long)seg * (a.N1 + 1);
-  const float mb = Mb ? Mb[n3 + n3off] : 1.f;
   __syncthreads();
   float2 acc[F1];
 #pragma unroll
   for (int m = 0; m < F1; ++m) acc[m] = make_float2(0.f, 0.f);
   for (int c = 0; c < a.C; c += 2) {
     const bool two = c + 1 < a.C;
-    const long long yo0 = ld * (n3 + n3off) + ld * N3y * c;
-    const long long yo1 = yo0 + ld * N3y;
+    // this (c, n3) row of the gathered samples, indexed by CSR position
+    const float2* yq0 = a.part + (((long long)slot * a.C + c) * a.N3c + n3) * a.ldp - rp[0];
+    const float2* yq1 = yq0 + (long long)a.N3c * a.ldp;
     // each row's LPB lines in two halves (rows first, so a warp's stores are
     // consecutive): a thread sums the row's samples into LPB / 2 lines
     constexpr int HL = LPB / 2;
@@ -255,15 +284,14 @@ __global__ void __launch_bounds__(kThreads, 2) sum_adj_kernel(SumArgs a, const f
       for (int q = rp[r]; q < qe; q += 2) {
         // two samples of the row at a time; a missing second one adds zeros
         const bool hb = q + 1 < qe;
-        const int i0 = a.perm[q], i1 = hb ? a.perm[q + 1] : i0;
+        const float2 zero = make_float2(0.f, 0.f);
         const int kz0 = a.kzq[q], kz1 = hb ? a.kzq[q + 1] : kz0;
-        const float wt0 = We ? mb * We[i0] : mb, wt1 = hb ? (We ? mb * We[i1] : mb) : 0.f;
         const float2 w0 = tws[(int)(((long long)kz0 * (b0 + jb)) % a.N2)], st0 = tws[kz0];
         const float2 w1 = tws[(int)(((long long)kz1 * (b0 + jb)) % a.N2)], st1 = tws[kz1];
-        const float2 p0 = cmul(cscale(y[yo0 + i0], wt0), w0);
-        const float2 p1 = two ? cmul(cscale(y[yo1 + i0], wt0), w0) : make_float2(0.f, 0.f);
-        const float2 r0 = cmul(cscale(y[yo0 + i1], wt1), w1);
-        const float2 r1 = two ? cmul(cscale(y[yo1 + i1], wt1), w1) : make_float2(0.f, 0.f);
+        const float2 p0 = cmul(yq0[q], w0);
+        const float2 p1 = two ? cmul(yq1[q], w0) : zero;
+        const float2 r0 = hb ? cmul(yq0[q + 1], w1) : zero;
+        const float2 r1 = (hb && two) ? cmul(yq1[q + 1], w1) : zero;
         float2 VX = make_float2(p0.x, p1.x), VY = make_float2(p0.y, p1.y);
         float2 UX = make_float2(r0.x, r1.x), UY = make_float2(r0.y, r1.y);
         const float2 SX0 = bc(st0.x), SY0 = bc(st0.y), SN0 = bc(-st0.y);
@@ -335,12 +363,11 @@ struct SumLaunch {
     sum_fwd_kernel<F1, F2><<<grid, kThreads, smem(), s>>>(a, z, tw);
     return true;
   }
-  static bool adj(const SumArgs& a, const float2* y, long long ld, int n3off, int N3y, const float* We,
-                  const float* Mb, float2* u, float scale, const float2* tw, cudaStream_t s) {
+  static bool adj(const SumArgs& a, float2* u, float scale, const float2* tw, cudaStream_t s) {
     static const bool ok = init();
     if (!ok) return false;
     const unsigned grid = (unsigned)(((long long)a.N2 * a.N3c / LPB) * a.n_slots);
-    sum_adj_kernel<F1, F2><<<grid, kThreads, smem(), s>>>(a, y, ld, n3off, N3y, We, Mb, u, scale, tw);
+    sum_adj_kernel<F1, F2><<<grid, kThreads, smem(), s>>>(a, u, scale, tw);
     return true;
   }
 };
@@ -428,15 +455,23 @@ int dis_coil_sum_fwd(disorder_ctx_s* ctx, const disorder_plan_s* plan, const Coi
   return DISORDER_OK;
 }
 
+// bytes of the adjoint's gathered samples per slot
+size_t dis_sum_gather_bytes(int C, int N3c, int ldq) { return (size_t)C * N3c * (size_t)ldq * sizeof(float2); }
+
 // decode's coil stage: u (slot volumes, first readout row of the chunk) from
-// the samples y weighted by We (per sample) and Mb (per readout row)
+// the samples y weighted by We (per sample) and Mb (per readout row); yq:
+// dis_sum_gather_bytes per slot of scratch, ldq the most samples of a segment
 int dis_coil_sum_adj(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CoilArgs& a, const float2* y,
-                     long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* u, float scale) {
+                     long long y_ld, int y_n3off, int y_N3, const float* We, const float* Mb, float2* u, float scale,
+                     float2* yq, int ldq) {
   if (a.n_slots == 0 || a.N3c == 0) return DISORDER_OK;
-  const sc::SumArgs s = sum_args(plan, a, nullptr, 0);
-  const bool ok = sc::dispatch(a.N1, [&](auto L) {
-    return decltype(L)::adj(s, y, y_ld, y_n3off, y_N3, We, Mb, u, scale, plan->d_tw[0], ctx->stream);
-  });
+  if (!yq || ldq < 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "sample-sum adjoint: no sample scratch");
+  const sc::SumArgs s = sum_args(plan, a, yq, ldq);
+  const long long tot = (long long)a.n_slots * a.C * a.N3c * ldq;
+  const int blocks = (int)std::min<long long>((tot + 255) / 256, 8LL * ctx->sm_count);
+  sc::sum_gather_kernel<<<std::max(blocks, 1), 256, 0, ctx->stream>>>(s, y, y_ld, y_n3off, y_N3, We, Mb);
+  dis_count(ctx);
+  const bool ok = sc::dispatch(a.N1, [&](auto L) { return decltype(L)::adj(s, u, scale, plan->d_tw[0], ctx->stream); });
   if (!ok) return dis_set_error(ctx, DISORDER_BAD_ARG, "sample-sum coil stage: no kernel for N1=%d", a.N1);
   dis_count(ctx);
   DIS_CUDA_TRY(cudaGetLastError());
