@@ -648,6 +648,45 @@ def transform_roofline(ctx, cfg, sc, peak, pkind, reps=5):
                       "%d states, CUDA events, mean of %d" % (S, reps)}
 
 
+# ---------------------------------------------------------------- either side of the path
+def io_and_sampling(x, N, shots):
+    """The data formats either side of the reconstruction: the image written
+    as NIfTI (magnitude and phase files, IO/writeNII.m) and read back
+    (IO/readNII.m) through a temporary directory, with the device-to-host
+    copy included; and the acquisition-side DISORDER trajectory
+    (Acquisition/samplingDISORDER.m, random-checkered, alternating zig-zag)
+    of the scan's N1 x N2 phase-encode grid into the scan's shots. Wall
+    times on the host."""
+    import shutil
+    from disorder_b200 import nifti, sampling
+    d = tempfile.mkdtemp(prefix="disorder_io_")
+    try:
+        dat = os.path.join(d, "rec")
+        t0 = time.perf_counter()
+        nifti.writeNII(dat, ["Aq"], [x])
+        t_w = time.perf_counter() - t0
+        nbytes = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+        t0 = time.perf_counter()
+        y, _, _ = nifti.readNII(dat, ["Aq"])
+        t_r = time.perf_counter() - t0
+        xh = x.numpy()
+        err = float(np.linalg.norm(y[0] - xh) / np.linalg.norm(xh))
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    U = int(round(math.sqrt(shots)))
+    pts = sampling.cartesian_points(N[:2])
+    t0 = time.perf_counter()
+    _, NP, _, _, Shot, _ = sampling.samplingDISORDER(pts, (U, U), "RandomCheckered", "AlternatingZigZag",
+                                                     rng=np.random.default_rng(0))
+    t_s = time.perf_counter() - t0
+    return {"nifti": {"write_s": t_w, "read_s": t_r, "bytes": int(nbytes), "write_GBps": nbytes / t_w / 1e9,
+                      "read_GBps": nbytes / t_r / 1e9, "roundtrip_rel_err": err,
+                      "files": "magnitude + phase float32 NIfTI-1 of %s" % "x".join(map(str, N))},
+            "sampling": {"s": t_s, "points": int(NP), "shots": int(Shot.max()),
+                         "workload": "samplingDISORDER of the %dx%d grid, %dx%d tiles, random-checkered"
+                                     % (N[0], N[1], U, U)}}
+
+
 # ---------------------------------------------------------------- ranks
 def replica_seed(seed, rank):
     """Each replica reconstructs its own scan: the synthetic seed moves with the rank."""
@@ -889,6 +928,8 @@ def main():
                    "phases_s": {k: round(v, 4) for k, v in e2e_phases.items()}, "clocks": e2e_clocks},
            "roofline": roof, "roofline_mixed": roof_m, "roofline_transform": roof_t}
     out.update(variants)
+    if rank == 0:
+        out["io"] = io_and_sampling(head["x"], cfg["N"], cfg["shots"])
     if rank == 0 and not args.no_batch:
         # free the benchmark scan first: the batch holds about 45 GB of scans
         del sc

@@ -89,6 +89,7 @@ SIGNATURES = [
     ("disorder_synth_phantom", C.c_int, [VP, C.POINTER(I32), I32, FP, I32, FP, I32, VP]),
     ("disorder_synth_coils", C.c_int, [VP, C.POINTER(I32), I32, FP, C.c_float, VP]),
     ("disorder_add_noise", C.c_int, [VP, VP, C.c_int64, C.c_float, C.c_uint64]),
+    ("disorder_electrostatic_order", C.c_int, [I32, I32, C.POINTER(C.c_int32)]),
     ("disorder_net_param_count", C.c_int64, []),
     ("disorder_net_create", C.c_int, [VP, C.POINTER(I32), I32, C.POINTER(VP)]),
     ("disorder_net_destroy", C.c_int, [VP]),

@@ -360,6 +360,14 @@ int disorder_add_noise(disorder_ctx ctx, void* y, int64_t n, float sigma, uint64
  * grid and outputs 3-5 rotation updates / 8 degrees.
  * D: input volume size (n1, n2, n3); max_batch: most volumes per call. */
 typedef struct disorder_net_s* disorder_net;
+/* ---- sample orders (Acquisition/samplingDISORDER.m) ----
+ * The order in which samplingDISORDER.m:104 distributes a tile's n1 x n2
+ * positions over consecutive segments: Acquisition/
+ * electrostaticRepulsionDISORDER.m:9-52 (greedy minimum wrapped electric
+ * repulsion, first minimum by more than 1e-9 in column-major scan order).
+ * order: n1*n2 0-based column-major positions. Host computation; no context. */
+int disorder_electrostatic_order(int32_t n1, int32_t n2, int32_t* order);
+
 int64_t disorder_net_param_count(void);
 int disorder_net_create(disorder_ctx ctx, const int32_t* D, int32_t max_batch, disorder_net* net);
 int disorder_net_destroy(disorder_net net);
