@@ -928,14 +928,16 @@ def main():
                    "phases_s": {k: round(v, 4) for k, v in e2e_phases.items()}, "clocks": e2e_clocks},
            "roofline": roof, "roofline_mixed": roof_m, "roofline_transform": roof_t}
     out.update(variants)
-    if rank == 0:
+    # the single-GPU extras (data formats, batch of uneven scans, CPU
+    # baseline, config 1) run at N = 1 only
+    if world == 1:
         out["io"] = io_and_sampling(head["x"], cfg["N"], cfg["shots"])
-    if rank == 0 and not args.no_batch:
+    if world == 1 and not args.no_batch:
         # free the benchmark scan first: the batch holds about 45 GB of scans
         del sc
         os.environ["DISORDER_WORKSPACE_GB"] = "12"
         out["batch"] = batch_arm()
-    if rank == 0 and not args.no_cpu:
+    if world == 1 and not args.no_cpu:
         est, thr, desc, errs = cpu_estimate(cfg["N"], cfg["shots"], cfg["coils_kept"], counts, ctx=ctx)
         out["cpu_baseline"] = {"value": est, "unit": "s", "cores": thr, "kind": "port", "sample": desc}
         out["oracle_rel_err"] = errs

@@ -81,3 +81,14 @@ def test_bad_arguments():
         ps.samplingDISORDER(pts, (4, 4), "Spiral")
     with pytest.raises(ValueError):
         ps.samplingDISORDER(pts[:-1], (4, 4), "Checkered", "ZigZag")
+
+
+def test_electrostatic_order_rejects_bad_sizes():
+    import ctypes as C
+    from disorder_b200 import _lib
+    out = np.zeros(4, np.int32)
+    p = out.ctypes.data_as(C.POINTER(C.c_int32))
+    lib = _lib.load()
+    assert lib.disorder_electrostatic_order(0, 4, p) == 1  # DISORDER_BAD_ARG
+    assert lib.disorder_electrostatic_order(2, 2, None) == 1
+    assert lib.disorder_electrostatic_order(2, 2, p) == 0 and sorted(out.tolist()) == [0, 1, 2, 3]
