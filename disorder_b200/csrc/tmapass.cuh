@@ -168,6 +168,44 @@ __global__ void __launch_bounds__(kThreads, 3)
     const int w = KIND >= 1 ? it.slot * C + c : (shared_input ? 0 : it.slot);
     tma_load_tile(st, &in_map, it.ca, t.axis == 2 ? it.cb : 0, t.axis == 1 ? it.cb : 0, w, bar);
   };
+  // KIND 1 (with samples) / 2: the tile's samples of the forward DFT, warp
+  // by warp from registers. A warp holds two lines (16 threads each); the
+  // sample at (line, kz) is X[kz / F1] of lane 16 (line & 1) + kz % F1, so
+  // each lane takes one of the warp's samples (the segment's CSR over the two
+  // ky rows) and reads it with shuffles; no CTA barrier, no copy of the tile.
+  auto warp_samples = [&](const PItem& it, int c, float2 (&Xr)[F2], const float2* ymeas, float scale) {
+    if (lt >= F1) {
+#pragma unroll
+      for (int k2 = 0; k2 < F2; ++k2) Xr[k2] = make_float2(0.f, 0.f);
+    }
+    const int lane = tid & 31, wl0 = (tid >> 5) * 2;
+    const int* rp = t.rowptr + (long long)t.slot_seg[it.slot] * (t.Nv[0] + 1);
+    const int qa = rp[it.ca + min(wl0, it.nv)], qe = rp[it.ca + min(wl0 + 2, it.nv)];
+    const long long ob = t.ld * (it.cb + t.n3off) + t.ld * t.N3y * c;
+    for (int qb = qa; qb < qe; qb += 32) {
+      const int q = qb + lane;
+      const bool have = q < qe;
+      int i = 0, src = 0, kk = -1;
+      if (have) {
+        i = t.perm[q];
+        const int kz = t.kzv[i];
+        src = 16 * (t.kyv[i] - it.ca - wl0) + kz % F1;
+        kk = kz / F1;
+      }
+      float2 val = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int k2 = 0; k2 < F2; ++k2) {
+        const float vx = __shfl_sync(0xffffffffu, Xr[k2].x, src);
+        const float vy = __shfl_sync(0xffffffffu, Xr[k2].y, src);
+        if (kk == k2) val = make_float2(vx, vy);
+      }
+      if (have) {
+        float2 o = cscale(val, scale);
+        if (ymeas) o = csub(o, ymeas[ob + i]);
+        t.y[ob + i] = o;
+      }
+    }
+  };
   PItem cur;
   unit(b / S, b % S, cur);
   int cc = 0;
@@ -244,18 +282,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         for (int m = 0; m < F1; ++m) v[m] = (lt < F2) ? st[tswz(lt + F2 * m, li)] : make_float2(0.f, 0.f);
         __syncthreads();  // the tile becomes the exchange area
         LN::fwd(v, X, lt, myex, tw);
-        __syncthreads();  // every line's exchange is done
-        if (lt < F1) {
-#pragma unroll
-          for (int k2 = 0; k2 < F2; ++k2) st[tswz(lt + F1 * k2, li)] = X[k2];
-        }
-        __syncthreads();
-        for (int q = s0 + tid; q < s1; q += kThreads) {
-          const int i = t.perm[q];
-          float2 val = cscale(st[tswz(t.kzv[i], t.kyv[i] - cur.ca)], t.scale);
-          if (t.ymeas) val = csub(val, t.ymeas[ob + i]);
-          t.y[ob + i] = val;
-        }
+        warp_samples(cur, cc, X, t.ymeas, t.scale);
         cur = nxt;
         cc = cn;
         continue;
@@ -286,22 +313,8 @@ __global__ void __launch_bounds__(kThreads, 3)
     for (int m = 0; m < F1; ++m) v[m] = (lt < F2) ? st[tswz(lt + F2 * m, li)] : make_float2(0.f, 0.f);
     __syncthreads();  // the tile becomes the exchange area
     LN::fwd(v, X, lt, myex, tw);
-    if (KIND == 1 && t.y) {
-      // the segment's samples of this tile, as encode's gather writes them
-      __syncthreads();  // every line's exchange is done
-      if (lt < F1) {
-#pragma unroll
-        for (int k2 = 0; k2 < F2; ++k2) st[tswz(lt + F1 * k2, li)] = X[k2];
-      }
-      __syncthreads();
-      const int* rp = t.rowptr + (long long)t.slot_seg[cur.slot] * (t.Nv[0] + 1);
-      const long long ob = t.ld * (cur.cb + t.n3off) + t.ld * t.N3y * cc;
-      for (int q = rp[cur.ca] + tid; q < rp[cur.ca + cur.nv]; q += kThreads) {
-        const int i = t.perm[q];
-        t.y[ob + i] = cscale(st[tswz(t.kzv[i], t.kyv[i] - cur.ca)], t.scale);
-      }
-      __syncthreads();  // the tile is the exchange area again
-    }
+    // the segment's samples of this tile, as encode's gather writes them
+    if (KIND == 1 && t.y) warp_samples(cur, cc, X, nullptr, t.scale);
     if (lt < F1) {
       if (KIND == 0) {
         constexpr int KP = F2 / 2;
