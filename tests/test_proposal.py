@@ -215,11 +215,14 @@ def test_propose_step_never_raises_a_state_energy(ctx):
 
 
 @pytest.mark.gpu
-def test_trained_network_gain_over_the_plain_method(ctx):
-    """What the shipped network gains: on the training script's validation
-    scans (seed 5001) its loss against the zero proposal, and at the coarsest
-    level the motion error with and without the proposal after 9 outer
-    iterations (the proposal may not make it worse)."""
+def test_trained_network_predicts_motion_without_costing_accuracy(ctx):
+    """What the shipped network does: on the training script's validation
+    scans (seed 5001) its loss is below the zero proposal's (it predicts part
+    of the motion error), and at the coarsest level the motion error after 9
+    outer iterations with the gated proposal is within 0.25 voxel and 0.5
+    degree of the plain method's. It gains the plain method no iterations and
+    no time on these scans (the outer loop converges in the same 9 steps);
+    the printed figures show by how much it differs."""
     import os
     from disorder_b200 import proposal as pr
     if not os.path.exists(pr.WEIGHTS):
