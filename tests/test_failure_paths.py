@@ -90,6 +90,44 @@ def test_tma_wait_that_runs_out_is_reported_and_the_context_recovers(ctx):
 
 
 @pytest.mark.gpu
+def test_tensor_core_pass_wait_that_runs_out_is_reported(ctx):
+    """The same injected fault on a tensor-core (BF16x3) line pass: its tile
+    wait runs out before any MMA is issued, the kernel frees its tensor
+    memory and stops, and the context gives the clean result afterwards."""
+    import disorder_b200 as db
+    from disorder_b200 import _lib, api, synth
+    N, S = (16, 256, 16), 2  # 256-point strided lines: the tensor-core pass
+    rng = np.random.default_rng(31)
+    x = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    T = np.asfortranarray(synth.motion(S, 4.0, 2.0, rng))
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    grids = db.generateTransformGrids(N, N, cent)
+    plan = api._transform_plan(ctx, grids)
+    xd, out = ctx.upload(x), ctx.empty(N + (S,))
+    Tp = T.ctypes.data_as(_lib.FP)
+    L = ctx.lib
+    ctx.set_precision("bf16x3")
+    try:
+        assert L.disorder_ctx_inject_fault(ctx.h, 1) == 0
+        assert L.disorder_sinc_rigid_transform(ctx.h, plan.h, xd.ptr, 1, Tp, S, 1, 1, 1, out.ptr) == 0
+        assert L.disorder_synchronize(ctx.h) == 5  # DISORDER_TIMEOUT
+        assert b"ran out" in L.disorder_last_error(ctx.h)
+        ctx.check(L.disorder_sinc_rigid_transform(ctx.h, plan.h, xd.ptr, 1, Tp, S, 1, 1, 1, out.ptr))
+        assert L.disorder_synchronize(ctx.h) == 0
+        y1 = out.numpy()
+        ctx.check(L.disorder_sinc_rigid_transform(ctx.h, plan.h, xd.ptr, 1, Tp, S, 1, 1, 1, out.ptr))
+        assert L.disorder_synchronize(ctx.h) == 0
+        y2 = out.numpy()
+    finally:
+        ctx.set_precision("fp32")
+    assert np.array_equal(y1, y2)
+    et, _ = db.precomputeFactorsSincRigidTransform(grids, T, 1)
+    ref, _ = db.sincRigidTransform(x, et, 1, ctx=ctx)
+    err = np.linalg.norm(y1 - ref) / np.linalg.norm(ref)
+    assert 1e-7 < err < 1e-4  # the BF16x3 result (not the FP32 one)
+
+
+@pytest.mark.gpu
 def test_injected_allocation_failure_returns_oom():
     import disorder_b200 as db
     from conftest import make_problem
