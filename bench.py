@@ -10,6 +10,15 @@ resolution pyramid (64x64x44, 128x128x88, 256x256x176) with up to 20 outer
 iterations of CG + Levenberg-Marquardt motion estimation at the two coarse
 levels and a final CG (energy tolerance 1e-3) at full resolution.
 
+The headline (`value`) reconstructs with the learned motion proposal and the
+BF16x3 tensor-core DFT passes and Gram, as the metric names; the plain FP32
+method runs the same way beside it (`plain`, whose NRMSE is the target), each
+half alone once (`learned`, `mixed`), the headline from host arrays (`e2e`),
+the normal operator's roofline, the per-stage error against the FP64 oracle,
+and at N = 1 the data formats either side of the path (`io`), the batch of
+uneven scans (`batch`), the CPU baseline and the small case run in full on
+both (`config1`). `--plain` makes the plain method the headline.
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 For N > 1 (one process per GPU under torchrun) each GPU reconstructs its own
 scan (replicas; the path's multi-GPU shot sharding is not built): value is
