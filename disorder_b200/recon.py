@@ -13,12 +13,58 @@ leff >= 0 on, the image updates weight the shots by the outlier rejection
 Gibbs/B-spline filters of the reference driver are not part of this path.
 """
 
+import json
 import math
+import os
+import shutil
 import time
 
 import numpy as np
 
 from . import api
+
+# ---------------------------------------------------------------- checkpoints
+CHECKPOINT_VERSION = 1
+
+
+def save_state(path, meta, arrays):
+    """Write a checkpoint directory: state.json (the scalars in `meta`, and
+    for each array its file, dtype, shape and order) and one raw
+    little-endian file per array in column-major order (readable by
+    numpy.fromfile and MATLAB fread). The directory is replaced as a whole:
+    the new state is written beside it and renamed into place."""
+    tmp = path + ".tmp"
+    shutil.rmtree(tmp, ignore_errors=True)
+    os.makedirs(tmp)
+    files = {}
+    for name, a in arrays.items():
+        if a is None:
+            continue
+        a = a.numpy() if hasattr(a, "numpy") else np.asarray(a)
+        with open(os.path.join(tmp, name + ".raw"), "wb") as f:
+            f.write(np.asfortranarray(a.astype(a.dtype.newbyteorder("<"))).tobytes(order="F"))
+        files[name] = {"file": name + ".raw", "dtype": a.dtype.name, "shape": list(a.shape), "order": "F"}
+    with open(os.path.join(tmp, "state.json"), "w") as f:
+        json.dump(dict(meta, version=CHECKPOINT_VERSION, arrays=files), f, indent=1)
+    old = path + ".old"
+    shutil.rmtree(old, ignore_errors=True)
+    if os.path.exists(path):
+        os.rename(path, old)
+    os.rename(tmp, path)
+    shutil.rmtree(old, ignore_errors=True)
+
+
+def load_state(path):
+    """(meta, {name: array}) of a checkpoint written by save_state."""
+    with open(os.path.join(path, "state.json")) as f:
+        meta = json.load(f)
+    if meta.get("version") != CHECKPOINT_VERSION:
+        raise ValueError("checkpoint %s: version %r, expected %d" % (path, meta.get("version"), CHECKPOINT_VERSION))
+    arrays = {}
+    for name, d in meta["arrays"].items():
+        a = np.fromfile(os.path.join(path, d["file"]), dtype=np.dtype(d["dtype"]).newbyteorder("<"))
+        arrays[name] = a.reshape(d["shape"], order="F").astype(d["dtype"])
+    return meta, arrays
 
 
 def pyramidPlan(voxSiz, resolMax=4.0, NWend=1, accel=(1, 0)):
@@ -271,7 +317,8 @@ def alternating_reconstruction(ctx, S, y, ky, kz, nEc, mSt, n_states, N, n_outer
 
 def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), perc=16, resolMax=4.0,
                            nExtern=20, winit=1e-3, traLimXT=(0.05, 0.02), redFOV=1.0 / 3, echoesMin=4,
-                           tolerSolve=1e-3, log=None, proposal=None, levels=None, traLimX=(0.05, 0.02), outliers=True):
+                           tolerSolve=1e-3, log=None, proposal=None, levels=None, traLimX=(0.05, 0.02), outliers=True,
+                           checkpoint=None, resume=False, stop_after=None):
     """Motion-corrected reconstruction of one scan on the GPU.
 
     S: coil maps (N1,N2,N3,C) device array; y: samples (Ns,N3,C) device array
@@ -286,7 +333,15 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
     image update (compressMotion; None: no binning). outliers: the shot
     weights of the outlier rejection (rec.Alg.AlignedRec=2, solveXT.m:440-482),
     computed after each image update at the levels with leff >= 0 and applied
-    to the later image updates of that level and to the final one. Returns (x device volume, T (n_states, 6), log).
+    to the later image updates of that level and to the final one.
+    checkpoint: a directory that holds the latest state (save_state): after
+    every outer iteration of a level its image, motion, LM damping and
+    convergence flags, reset counters and shot weights; after every level
+    the full-size image. resume: continue from that state (the result is the
+    one the run without a stop gives). stop_after = (level, iteration) returns
+    right after the checkpoint of that outer iteration, or of the end of the
+    level when iteration is None (a staged run, e.g. a job with a time limit).
+    Returns (x device volume, T (n_states, 6), log).
     """
     log = log if log is not None else ReconLog()
     N = tuple(int(n) for n in N)
@@ -302,11 +357,37 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
     n_coarse = int(np.sum(resPyr != 1))
     We_shot = None
     n_run = L if levels is None else min(L, levels)
-    for l in range(n_run):
+    start_level, mid = 0, None  # mid: a checkpoint taken inside a level
+    if checkpoint and resume and os.path.exists(os.path.join(checkpoint, "state.json")):
+        meta, arr = load_state(checkpoint)
+        if meta["N"] != list(N) or meta["n_states"] != n_states:
+            raise ValueError("checkpoint %s holds a %s scan with %d states" % (checkpoint, meta["N"], meta["n_states"]))
+        T = np.ascontiguousarray(arr["T"], np.float32)
+        We_shot = arr.get("We")
+        if meta["iteration"] is None:
+            start_level = meta["level"] + 1
+            x = ctx.upload(arr["x"])
+        else:
+            start_level, mid = meta["level"], (meta, arr)
+        log.add(step="resume", level=meta["level"], it=meta["iteration"])
+
+    def save(l, n, xs, E_=None, est_=None, nReset_=0, cont_=0):
+        if not checkpoint:
+            return
+        meta = {"N": list(N), "n_states": n_states, "level": l, "iteration": n, "est": est_, "nReset": nReset_,
+                "cont": cont_}
+        arrays = {"x": xs, "T": T if E_ is None else E_.Tr, "We": We_shot}
+        if E_ is not None:
+            arrays["w"] = np.asarray(E_.w, np.float32)
+            arrays["cT"] = np.asarray(E_.cT, np.uint8)
+        save_state(checkpoint, meta, arrays)
+
+    for l in range(start_level, n_run):
         leff = l + 1 - n_coarse  # solveXT.m:269
         NXres = tuple(int(math.ceil(n * resPyr[l])) for n in N)
         # level operators (downsampleOperators, solveXT.m:333-342)
-        xRes = api.resampling(x, NXres, ctx=ctx)
+        resumed = mid is not None and l == start_level
+        xRes = ctx.upload(mid[1]["x"]) if resumed else api.resampling(x, NXres, ctx=ctx)
         SRes = api.resampling(Sc, NXres, ctx=ctx)
         ky, kz, nEc, mSt, src = level_sampling(H, n_states, NXres[:2])
         empty = unsampled_states(nEc, n_states)
@@ -343,8 +424,15 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
         est = bool(estT[l])
         use_net = proposal is not None and est and tuple(NXres) == tuple(proposal.D)
         rres = None  # the sample residual of the image updates at the outlier levels
-        nReset, cont = 0, 0
-        for n in range(nExtern):
+        nReset, cont, n0 = 0, 0, 0
+        if resumed:
+            meta, arr = mid
+            E.w = arr["w"].astype(np.float32)
+            E.cT = arr["cT"].astype(bool)
+            est, nReset, cont, n0 = bool(meta["est"]), int(meta["nReset"]), int(meta["cont"]), int(meta["iteration"])
+            if outliers and leff >= 0 and l < n_run - 1 and We_shot is not None and np.any(We_shot < 1):
+                EH = api.Struct(Mbe=Mbe_d, We=_sample_weights(We_shot, mSt, n_states))
+        for n in range(n0, nExtern):
             if nReset == 0 or cont % nReset == 0 or np.all(E.cT):  # solveXT.m:379-384
                 nReset += 1
                 cont = 0
@@ -387,5 +475,13 @@ def aligned_reconstruction(ctx, S, y, H, n_states, N, voxSiz=(1.0, 1.0, 1.0), pe
                     energy=float(np.sum(E.En)))
             if np.all(E.cT):  # weak convergence (solveXT.m:530-534)
                 est = False
+            save(l, n + 1, xRes, E, est, nReset, cont)
+            if stop_after is not None and tuple(stop_after) == (l, n):
+                log.add(step="stopped", level=l, it=n)
+                return api.resampling(xRes, N, ctx=ctx), T, log
         x = api.resampling(xRes, N, ctx=ctx)
+        save(l, None, x)
+        if stop_after is not None and tuple(stop_after) == (l, None):
+            log.add(step="stopped", level=l)
+            return x, T, log
     return x, T, log
