@@ -8,7 +8,10 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdisorder.so")
+# DISORDER_LIB=checks loads the build with the device index checks
+# (python -m disorder_b200.build --debug)
+LIB_PATH = os.path.join(HERE, "libdisorder_checks.so" if os.environ.get("DISORDER_LIB") == "checks"
+                        else "libdisorder.so")
 
 STATUS = {0: "OK", 1: "BAD_ARG", 2: "UNSUPPORTED_FIELD", 3: "OOM", 4: "CUDA_ERR", 5: "TIMEOUT",
           6: "NONFINITE"}
@@ -110,7 +113,8 @@ def load():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise OSError("libdisorder.so not built (run python -m disorder_b200.build): %s" % LIB_PATH)
+            raise OSError("%s not built (run python -m disorder_b200.build%s)"
+                          % (LIB_PATH, " --debug" if LIB_PATH.endswith("_checks.so") else ""))
         lib = C.CDLL(LIB_PATH)
         for name, res, args in SIGNATURES:
             f = getattr(lib, name)

@@ -2,7 +2,11 @@
 
 Usage: python -m disorder_b200.build [--debug]
 Objects go to _build/ at the repository root; the shared library is written
-next to this file as disorder_b200/libdisorder.so.
+next to this file as disorder_b200/libdisorder.so. --debug builds the
+device index checks in (-DDISORDER_CHECKS: every checked index outside its
+array is recorded and skipped, and disorder_synchronize reports it) into
+disorder_b200/libdisorder_checks.so (objects in _build_checks/); the package
+loads it instead when DISORDER_LIB=checks.
 """
 
 import argparse
@@ -15,6 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdisorder.so")
+LIB_CHECKS = os.path.join(HERE, "libdisorder_checks.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -30,7 +35,8 @@ def nvcc():
 
 
 def build(debug=False, verbose=False, jobs=8):
-    bdir = os.path.join(ROOT, "_build")
+    bdir = os.path.join(ROOT, "_build_checks" if debug else "_build")
+    lib_out = LIB_CHECKS if debug else LIB
     os.makedirs(bdir, exist_ok=True)
     flags = ARCH + ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                     "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
@@ -60,12 +66,12 @@ def build(debug=False, verbose=False, jobs=8):
                 sys.stderr.write(r.stdout + r.stderr)
             if r.returncode:
                 raise RuntimeError("nvcc failed: " + " ".join(cmd))
-    link = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+    link = [nvcc()] + ARCH + ["-shared", "-o", lib_out] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"]
     r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
-    return LIB
+    return lib_out
 
 
 if __name__ == "__main__":

@@ -205,13 +205,16 @@ int disorder_synchronize(disorder_ctx ctx) {
   CTX_CHECK(ctx);
   DEV_GUARD(ctx);
   DIS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  // a bounded in-kernel wait that ran out (the kernel stopped early)
-  int err = 0;
-  DIS_CUDA_TRY(cudaMemcpy(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (err) {
-    DIS_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(int)));
+  // err[0]: a bounded in-kernel wait that ran out (the kernel stopped early);
+  // err[1]: the site of a device index check that failed (the access skipped)
+  int err[2] = {0, 0};
+  DIS_CUDA_TRY(cudaMemcpy(err, ctx->d_err, sizeof(err), cudaMemcpyDeviceToHost));
+  if (err[0] || err[1]) DIS_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(err)));
+  if (err[0])
     return dis_set_error(ctx, DISORDER_TIMEOUT, "a TMA tile wait in a line pass ran out; results are incomplete");
-  }
+  if (err[1])
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "a device index check failed (site %d): an index outside its "
+                         "array was skipped; results are incomplete", err[1]);
   return DISORDER_OK;
 }
 

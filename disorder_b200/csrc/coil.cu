@@ -252,9 +252,13 @@ __global__ void __launch_bounds__(kThreads) ifft1_combine_kernel(CoilArgs a, con
 
 __global__ void weight_map_kernel(const int* __restrict__ segof, const int* __restrict__ kyv,
                                   const int* __restrict__ kzv, const float* __restrict__ We, long long ns,
-                                  int N1, int N2, float* __restrict__ wmap, float scale) {
+                                  int N1, int N2, float* __restrict__ wmap, float scale, int n_seg,
+                                  int* __restrict__ err) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
     const float w = (We ? We[i] : 1.f) * scale;
+    if (!DIS_DEBUG_INDEX(segof[i], n_seg, err, DIS_SITE_WEIGHT_MAP) || !DIS_DEBUG_INDEX(kyv[i], N1, err, DIS_SITE_WEIGHT_MAP) ||
+        !DIS_DEBUG_INDEX(kzv[i], N2, err, DIS_SITE_WEIGHT_MAP))
+      continue;
     atomicAdd(&wmap[((long long)segof[i] * N1 + kyv[i]) * N2 + kzv[i]], w);
   }
 }
@@ -424,7 +428,7 @@ int dis_build_weight_map(disorder_ctx_s* ctx, const disorder_plan_s* plan, const
   if (plan->n_samples == 0) return DISORDER_OK;
   const int blocks = (int)std::min<long long>((plan->n_samples + 255) / 256, 4096);
   weight_map_kernel<<<blocks, 256, 0, ctx->stream>>>(plan->d_seg_of, plan->d_ky, plan->d_kz, We, plan->n_samples,
-                                                     plan->N[0], plan->N[1], wmap, scale);
+                                                     plan->N[0], plan->N[1], wmap, scale, plan->n_seg, ctx->d_err);
   dis_count(ctx);
   DIS_CUDA_TRY(cudaGetLastError());
   return DISORDER_OK;

@@ -9,6 +9,24 @@
 #define DIS_HD __host__ __device__ __forceinline__
 #define DIS_D __device__ __forceinline__
 
+// Device-side index checks. dis_index_ok is false when i lies outside
+// [0, n): it records `site` in err[1] (the context's device error word; the
+// first failing site wins) and the caller skips the access, so a bad index
+// never reaches memory. disorder_synchronize reports it as BAD_ARG. Indices
+// that come from the caller are always checked; DIS_DEBUG_INDEX checks the
+// library's own (plan-derived) indices only in a -DDISORDER_CHECKS build.
+enum DisCheckSite { DIS_SITE_GATHER_ROWS = 1, DIS_SITE_WEIGHT_MAP = 2, DIS_SITE_TMA_SAMPLES = 3 };
+__device__ __forceinline__ bool dis_index_ok(long long i, long long n, int* err, int site) {
+  if (i >= 0 && i < n) return true;
+  if (err) atomicCAS(err + 1, 0, site);
+  return false;
+}
+#ifdef DISORDER_CHECKS
+#define DIS_DEBUG_INDEX(i, n, err, site) dis_index_ok((i), (n), (err), (site))
+#else
+#define DIS_DEBUG_INDEX(i, n, err, site) true
+#endif
+
 DIS_HD float2 c2(float x, float y) { return make_float2(x, y); }
 // Complex add/subtract. On sm_100 one packed add.f32x2 / sub.f32x2 does both
 // lanes (round-to-nearest per lane, the same results as two scalar ops).

@@ -95,12 +95,17 @@ __global__ void __launch_bounds__(kThreads) resample_kernel(ResampleArgs a) {
   }
 }
 
+// the caller's indices are checked: one outside [0, ld_in) gives a zero row
+// and the site in the error word, never an out-of-bounds read
 __global__ void gather_rows_kernel(const float2* __restrict__ in, long long ld_in, const int* __restrict__ idx,
-                                   long long n_out, long long rows, float scale, float2* __restrict__ out) {
+                                   long long n_out, long long rows, float scale, float2* __restrict__ out,
+                                   int* __restrict__ err) {
   const long long tot = n_out * rows;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
     const long long i = e % n_out, r = e / n_out;
-    out[e] = cscale(in[idx[i] + ld_in * r], scale);
+    const int k = idx[i];
+    out[e] = dis_index_ok(k, ld_in, err, DIS_SITE_GATHER_ROWS) ? cscale(in[k + ld_in * r], scale)
+                                                               : make_float2(0.f, 0.f);
   }
 }
 
@@ -328,7 +333,7 @@ int disorder_gather_samples(disorder_ctx ctx, const void* y_in, int64_t n_in, in
   const long long tot = n_out * rows;
   const int blocks = (int)std::min<long long>((tot + 255) / 256, 16LL * ctx->sm_count);
   gather_rows_kernel<<<blocks, 256, 0, ctx->stream>>>((const float2*)y_in, n_in, idx, n_out, rows, scale,
-                                                      (float2*)y_out);
+                                                      (float2*)y_out, ctx->d_err);
   dis_count(ctx);
   DIS_CUDA_TRY(cudaGetLastError());
   return DISORDER_OK;

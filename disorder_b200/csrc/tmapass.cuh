@@ -188,9 +188,12 @@ __global__ void __launch_bounds__(kThreads, 3)
       int i = 0, src = 0, kk = -1;
       if (have) {
         i = t.perm[q];
-        const int kz = t.kzv[i];
-        src = 16 * (t.kyv[i] - it.ca - wl0) + kz % F1;
-        kk = kz / F1;
+        const int kz = t.kzv[i], row = t.kyv[i] - it.ca - wl0;
+        if (DIS_DEBUG_INDEX(kz, t.Nv[t.axis], t.err, DIS_SITE_TMA_SAMPLES) &&
+            DIS_DEBUG_INDEX(row, 2, t.err, DIS_SITE_TMA_SAMPLES)) {
+          src = 16 * row + kz % F1;
+          kk = kz / F1;
+        }
       }
       float2 val = make_float2(0.f, 0.f);
 #pragma unroll
@@ -299,6 +302,9 @@ __global__ void __launch_bounds__(kThreads, 3)
         const int i = t.perm[q];
         const float w = t.We ? mb * t.We[i] : mb;
         const float2 val = cscale(t.y[ob + i], w);
+        if (!DIS_DEBUG_INDEX(t.kzv[i], t.Nv[t.axis], t.err, DIS_SITE_TMA_SAMPLES) ||
+            !DIS_DEBUG_INDEX(t.kyv[i] - cur.ca, cur.nv, t.err, DIS_SITE_TMA_SAMPLES))
+          continue;
         float2* d = &st[tswz(t.kzv[i], t.kyv[i] - cur.ca)];
         atomicAdd(&d->x, val.x);
         atomicAdd(&d->y, val.y);
