@@ -250,13 +250,33 @@ def _uncorrected(ctx, S, y, H, n_states, N, tolerSolve):
 
 
 class ReconLog:
-    def __init__(self):
+    """The structured log of a reconstruction: one event per step (cg, lm,
+    proposal, outliers, compress, resume, stopped, abort) with its level,
+    outer iteration, step figures (CG iterations, LM energy and unconverged
+    states, proposals kept, shots down-weighted) and the host time since the
+    start (the solver calls synchronise, so it includes their device time).
+    The figures the reference prints (CGsolver.m:88,102, LMsolver.m:198,
+    210-212) as JSON lines instead."""
+
+    def __init__(self, path=None):
         self.events = []
         self.t0 = time.perf_counter()
+        self.path = path  # when set, every event is appended to this file as one JSON line
 
     def add(self, **kw):
         kw["t"] = time.perf_counter() - self.t0
         self.events.append(kw)
+        if self.path:
+            with open(self.path, "a") as f:
+                f.write(json.dumps(kw, default=_json_default) + "\n")
+
+
+def _json_default(v):
+    if isinstance(v, np.generic):
+        return v.item()
+    if isinstance(v, np.ndarray):
+        return v.tolist()
+    raise TypeError("%r is not JSON serialisable" % type(v))
 
 
 def reset_schedule():

@@ -63,3 +63,15 @@ def test_staged_reconstruction_equals_the_uninterrupted_one(tmp_path, stop):
     assert any(e["step"] == "resume" for e in log2.events)
     assert np.array_equal(Tb, Ta)
     assert np.array_equal(xb.numpy(), xa.numpy())
+
+
+def test_log_events_as_json_lines(tmp_path):
+    from disorder_b200 import recon
+    path = str(tmp_path / "log.jsonl")
+    log = recon.ReconLog(path)
+    log.add(step="cg", level=0, it=1, iters=np.int64(3), energy=np.float32(2.5))
+    log.add(step="lm", level=0, it=1, unconverged=4, states=[1, 2])
+    lines = [json.loads(l) for l in open(path)]
+    assert [l["step"] for l in lines] == ["cg", "lm"]
+    assert lines[0]["iters"] == 3 and lines[0]["energy"] == 2.5 and lines[1]["states"] == [1, 2]
+    assert lines[1]["t"] >= lines[0]["t"] >= 0
