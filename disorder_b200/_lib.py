@@ -102,6 +102,16 @@ SIGNATURES = [
     ("disorder_net_backward", C.c_int, [VP, VP, VP, I32, VP, DP]),
     ("disorder_net_adam", C.c_int, [VP, VP, VP, C.c_float, C.c_float, C.c_float, C.c_float, I32]),
     ("disorder_propose_motion", C.c_int, [VP, VP, VP, VP, VP, I32, VP, FP, I32, I32, C.c_float, FP]),
+    ("disorder_shearlet_create", C.c_int, [VP, C.POINTER(I32), I32, VP, VP, VP, I32, C.POINTER(I32),
+                                           C.POINTER(VP)]),
+    ("disorder_shearlet_destroy", C.c_int, [VP]),
+    ("disorder_shearlet_coefficients", C.c_int, [VP, VP, VP, C.c_float, C.c_float, VP]),
+    ("disorder_shearlet_regularize", C.c_int, [VP, VP, VP, VP, C.c_float, C.c_float, VP]),
+    ("disorder_shearlet_trace", C.c_int, [VP, VP, VP, VP, DP]),
+    ("disorder_fidelity_trace", C.c_int, [VP, C.POINTER(I32), VP, VP, I32, VP, DP]),
+    ("disorder_cg_solve_shearlet", C.c_int, [VP, VP, VP, VP, I32, FP, VP, VP, VP, VP, VP, VP, VP, VP, C.c_float,
+                                             VP, I32, I32, I32, C.c_double, DP, C.POINTER(I32),
+                                             C.POINTER(I32)]),
 ]
 
 _lib = None

@@ -476,7 +476,15 @@ def CGsolver(y, E, EH, A=None, Cs=None, R=None, x=None, nIt=300, tolType="Energy
     ptr = lambda d: d.ptr if d is not None else None  # noqa: E731
     args = (ctx.h, p.h, yd.ptr, Sd.ptr, Cn, T[1] if T else None, ptr(We), ptr(Mb), ptr(Mbe), ptr(Se), ptr(Ma),
             ptr(Ti), xd.ptr, x_init, int(nIt), TOLTYPES[tolType], float(tol), En, C.byref(n_en), C.byref(nn))
-    if residual is not None:
+    if R is not None and R.has("Sh"):
+        # the shearlet term (Reconstruction/regularize.m:27-46): R.Sh holds the
+        # system (disorder_b200.cs.ShearletSystem), We, la and p
+        if residual is not None:
+            raise DisorderError(1, "CG with R.Sh does not return the sample residual")
+        sh = R.Sh
+        ctx.check(ctx.lib.disorder_cg_solve_shearlet(*args[:12], sh.sys.h, sh.We.ptr, float(sh.la * sh.p / 2),
+                                                     *args[12:]))
+    elif residual is not None:
         ctx.check(ctx.lib.disorder_cg_solve_residual(*args, residual.ptr))
     else:
         ctx.check(ctx.lib.disorder_cg_solve(*args))

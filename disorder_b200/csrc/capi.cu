@@ -703,3 +703,39 @@ int disorder_lm_step(disorder_ctx ctx, disorder_plan plan, const void* y, const 
 }
 
 }  // extern "C"
+
+int disorder_cg_solve_shearlet(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf, int32_t n_coils,
+                               const float* T, const float* We, const float* Mb, const float* Mbe, const float* P_Se,
+                               const float* C_Ma, const float* R_Ti, disorder_shearlet sh, const float* sh_We,
+                               float sh_scale, void* x_inout, int32_t x_init, int32_t nIt, int32_t tolType,
+                               double tol, double* En, int32_t* n_en, int32_t* nn) {
+  PLAN_CHECK(ctx, plan);
+  if (!y || !Sf || !x_inout || n_coils < 1 || nIt < 0 || !n_en || !nn || !sh || !sh_We)
+    return dis_set_error(ctx, DISORDER_BAD_ARG, "cg_solve_shearlet: bad arguments");
+  if (dis_shearlet_ctx(sh) != ctx) return dis_set_error(ctx, DISORDER_BAD_ARG, "cg_solve_shearlet: system of another context");
+  int shN[3];
+  dis_shearlet_size(sh, shN);
+  for (int m = 0; m < 3; ++m)
+    if (shN[m] != plan->N[m])
+      return dis_set_error(ctx, DISORDER_BAD_ARG, "cg_solve_shearlet: shearlet size %d x %d x %d != plan size",
+                           shN[0], shN[1], shN[2]);
+  CGSpec s;
+  s.y = (const float2*)y;
+  s.Sf = (const float2*)Sf;
+  s.C = n_coils;
+  s.T = T;
+  s.We = We;
+  s.Mb = Mb;
+  s.Mbe = Mbe;
+  s.P_Se = P_Se;
+  s.C_Ma = C_Ma;
+  s.R_Ti = R_Ti;
+  s.sh = sh;
+  s.sh_We = sh_We;
+  s.sh_scale = sh_scale;
+  int a = 0, b = 0;
+  const int st = dis_cg_solve(ctx, plan, s, (float2*)x_inout, x_init, nIt, tolType, tol, En, &a, &b);
+  *n_en = a;
+  *nn = b;
+  return st;
+}

@@ -442,6 +442,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   // EHE for the initial guess (:53-56)
   if (x_init) {
     if (!fused_init) DIS_TRY(normal_op(x, ehe, nullptr));
+    if (s.sh) DIS_TRY(dis_shearlet_regularize(ctx, s.sh, x, s.sh_We, s.sh_scale, 1.f, ehe));
     pap_kernel<<<blocks, 256, 0, ctx->stream>>>(x, ehe, s.C_Ma, s.R_Ti, V, R.part);
     dis_count(ctx);
     DIS_TRY(red_finish(R, &dummy, nullptr));
@@ -477,6 +478,7 @@ int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec&
   int n = 0;
   for (n = 1; n <= nIt; ++n) {
     DIS_TRY(normal_op(p, ehe, ebuf));  // :80 (and E p for the residual)
+    if (s.sh) DIS_TRY(dis_shearlet_regularize(ctx, s.sh, p, s.sh_We, s.sh_scale, 1.f, ehe));  // regularize.m:27-46
     pap_kernel<<<blocks, 256, 0, ctx->stream>>>(p, ehe, s.C_Ma, s.R_Ti, V, R.part);
     dis_count(ctx);
     double pa_re = 0, pa_im = 0;

@@ -14,6 +14,10 @@ struct CGSpec {
   const float* C_Ma = nullptr;
   const float* R_Ti = nullptr;
   float2* r_out = nullptr;  // device, optional: the final sample residual E x - y (encode's layout)
+  // shearlet term of regularize.m:27-46 (CSsolver.m:76): sh_scale = la p / 2
+  const disorder_shearlet_s* sh = nullptr;
+  const float* sh_We = nullptr;
+  float sh_scale = 0.f;
 };
 
 struct LMSpec {
@@ -25,6 +29,13 @@ struct LMSpec {
   float tL[2] = {0.f, 0.f};
   int n3_lo = 0, n3_hi = 0;
 };
+
+// out = beta out + scale IDFT3(sum_w S_w .* DFT3(We_w .* IDFT3(conj(S_w) .* DFT3(x)))) (shearlet.cu)
+int dis_shearlet_regularize(disorder_ctx_s* ctx, const disorder_shearlet_s* sh, const float2* x, const float* We,
+                            float scale, float beta, float2* out);
+
+disorder_ctx_s* dis_shearlet_ctx(const disorder_shearlet_s* sh);
+void dis_shearlet_size(const disorder_shearlet_s* sh, int* N);
 
 int dis_cg_solve(disorder_ctx_s* ctx, const disorder_plan_s* plan, const CGSpec& s, float2* x, int x_init, int nIt,
                  int tolType, double tol, double* En, int* n_en, int* nn);

@@ -402,6 +402,50 @@ int disorder_propose_motion(disorder_ctx ctx, disorder_plan plan, disorder_net n
                             const void* Sf, int32_t n_coils, const void* x, const float* T,
                             int32_t n3_lo, int32_t n3_hi, float gain, float* dT);
 
+/* ---- compressed-sensing reconstruction (Reconstruction/CSsolver.m) ----
+ * A shearlet system (Shearlets/buildShearlet.m, 3-D, complex=0) held as its
+ * 2-D planes: pair 0 = dims (1,2), pair 1 = dims (1,3), pair 2 = dims (3,2);
+ * 3-D shearlet w is plane table[4w+1] of pair table[4w] times plane
+ * table[4w+3] of pair table[4w+2] (buildShearlet.m:136-146). planesQ: host
+ * complex64, n_planes planes of N[a] x N[b] (column-major, a = first dim of
+ * the pair), frequency 0 first. Every N[m] must be a product of 2, 3, 5, 7,
+ * 11 and 13 (else DISORDER_UNSUPPORTED_FIELD). */
+typedef struct disorder_shearlet_s* disorder_shearlet;
+int disorder_shearlet_create(disorder_ctx ctx, const int32_t N[3], int32_t n_planes, const void* planes0,
+                             const void* planes1, const void* planes2, int32_t n_filters,
+                             const int32_t* table, disorder_shearlet* sh);
+int disorder_shearlet_destroy(disorder_shearlet sh);
+/* computeShearlet (CSsolver.m:91-101) and R.Sh.We=(R.Sh.We+eps).^pw
+ * (:59,80): We[w*V+v] = (|IDFT3(conj(S_w).*DFT3(x))|(v) + eps)^pw, with the
+ * unnormalised DFT of fftGPU and the 1/N inverse of ifftGPU. x: device V
+ * complex; We: device V x n_filters floats. */
+int disorder_shearlet_coefficients(disorder_ctx ctx, disorder_shearlet sh, const void* x, float eps,
+                                   float pw, float* We);
+/* Shearlet branch of regularize.m:27-46: out = beta*out + scale *
+ * IDFT3(sum_w S_w .* DFT3(We_w .* IDFT3(conj(S_w) .* DFT3(x)))), with
+ * scale = R.Sh.la*R.Sh.p/2. x, out: device V complex (out may not alias x). */
+int disorder_shearlet_regularize(disorder_ctx ctx, disorder_shearlet sh, const void* x, const float* We,
+                                 float scale, float beta, void* out);
+/* Regularizer term of traceEstimation.m:62-80 for one real probe:
+ * tr = sum_w ||sqrt(We_w) .* IDFT3(conj(S_w) .* DFT3(probe))||^2 (host). */
+int disorder_shearlet_trace(disorder_ctx ctx, disorder_shearlet sh, const float* probe, const float* We,
+                            double* tr);
+/* Fidelity term of traceEstimation.m:40-61 for one real probe:
+ * tr = sum_c sum_k W(k1,k2) |F2(S_c .* probe)(k)|^2, F2 the unitary DFT over
+ * dims 1-2 (fftGPU/sqrt(N)); W: device N1 x N2 weights (EH.We on the grid).
+ * Sf: device V x C complex. N1 and N2 as for shearlet_create. */
+int disorder_fidelity_trace(disorder_ctx ctx, const int32_t N[3], const float* probe, const void* Sf,
+                            int32_t C, const float* wgrid, double* tr);
+/* disorder_cg_solve with the shearlet term in the normal operator
+ * (CSsolver.m:76, CGsolver.m:55,80 calling regularize.m:27-46):
+ * EHE = constrain(encodedecode(p) + Ti.*p + scale*Sh(p; We)). */
+int disorder_cg_solve_shearlet(disorder_ctx ctx, disorder_plan plan, const void* y, const void* Sf,
+                               int32_t n_coils, const float* T, const float* We, const float* Mb,
+                               const float* Mbe, const float* P_Se, const float* C_Ma,
+                               const float* R_Ti, disorder_shearlet sh, const float* sh_We,
+                               float sh_scale, void* x_inout, int32_t x_init, int32_t nIt,
+                               int32_t tolType, double tol, double* En, int32_t* n_en, int32_t* nn);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,8 +2,8 @@
 
 TEST INFRASTRUCTURE ONLY. Restates Reconstruction/CGsolver.m:26-109,
 Reconstruction/stopCondition.m:10-21, Reconstruction/precondition.m:19-23
-(A.Se), Reconstruction/constrain.m:12 (C.Ma), Reconstruction/regularize.m:24
-(Tikhonov R.Ti) and Reconstruction/LMsolver.m:15-226 (the E.Fs branch, motion
+(A.Se), Reconstruction/constrain.m:12 (C.Ma), Reconstruction/regularize.m:24,27-46
+(Tikhonov R.Ti and the shearlet term R.Sh), Reconstruction/CSsolver.m:1-103 and Reconstruction/LMsolver.m:15-226 (the E.Fs branch, motion
 states along dim 5, one block of states).
 """
 
@@ -12,6 +12,7 @@ import itertools
 import numpy as np
 
 from . import encoding as enc
+from .shearlet import buildShearlet, compute_shearlet, regularize_sh, trace_estimation
 from .transform import (precomputeFactorsSincRigidTransform, restrictTransform,
                         sincRigidTransform, sincRigidTransformGradient)
 
@@ -44,10 +45,16 @@ def constrain(x, C):
 
 
 def regularize(x, R):
-    """Reconstruction/regularize.m:24 (Tikhonov R.Ti.la only)."""
-    if R is None or not R.has("Ti"):
-        return np.zeros_like(x)
-    return R.Ti * x
+    """Reconstruction/regularize.m:24 (Tikhonov, R.Ti = R.Ti.la) and :27-46
+    (shearlet, R.Sh with fields S, We, la, p)."""
+    out = np.zeros_like(x)
+    if R is not None and R.has("Ti"):
+        out = out + R.Ti * x
+    if R is not None and R.has("Sh"):
+        sh = R.Sh
+        x3 = x.reshape(x.shape[:3])
+        out = out + regularize_sh(x3, sh.S, sh.We, sh.la, sh.p).astype(out.dtype).reshape(out.shape)
+    return out
 
 
 def CGsolver(y, E, EH, A=None, C=None, R=None, x=None, nIt=300, tolType="Energy", tol=1e-5,
@@ -106,6 +113,50 @@ def CGsolver(y, E, EH, A=None, C=None, R=None, x=None, nIt=300, tolType="Energy"
     En = En[:, ::NitTest]
     return x, En, nn
 
+
+
+def CSsolver(y, E, EH, A=None, C=None, R=None, x=None, nIt=300, tolType="Energy", tol=1e-5, nOu=2, noise=None,
+             method="fft", dtype=np.float64):
+    """Reconstruction/CSsolver.m:21-89 (same grid in and out, so the
+    resampling steps :41-48,74 are identities). R.Ti is R.Ti.la and must be
+    given when C is empty (:47,72). noise(shape) draws the trace-estimation
+    probes. Returns (x, lambda)."""
+    from .encoding import Struct
+    if x is None:  # :33-38
+        EH0 = EH.copy(We=np.ones_like(np.asarray(EH.We, np.float64))) if EH.has("We") else EH
+        if EH0.has("Mbe"):
+            EH0 = EH0.copy(Mbe=np.ones_like(np.asarray(EH0.Mbe, np.float64)))
+        x, _, _ = CGsolver(y, E, EH0, A, C, R, None, nIt, tolType, tol, method, dtype)
+    if EH.has("Mbe"):
+        EH = EH.copy(Mbe=np.ones_like(np.asarray(EH.Mbe, np.float64)))
+    x = np.asarray(x)
+    NN = x.shape[:3]
+    if C is not None and C.has("Ma"):
+        C = C.copy(Ma=(np.asarray(C.Ma) > 0.5).astype(np.float64))  # :46
+    epsil, p = 1e-2, 1.0  # :51-53
+    S = buildShearlet(list(NN), 1, [1], "kos")["S"]  # :54
+    We = (compute_shearlet(x.reshape(NN), S) + epsil) ** (p - 2)  # :58-59
+    Sh = Struct(S=S, We=We, la=0.0, p=p)
+    Rr = (R or Struct()).copy(Sh=Sh)
+    trFid, _ = trace_estimation(x, E, EH, C, None, 1e-2, 4, noise)  # :63
+    trReg, _ = trace_estimation(x, None, None, C, Rr, 1e-2, 4, noise)  # :64
+    la = (2 / p) * trFid / (trReg + EPS)  # :65
+    lam = [la]
+    for n in range(1, nOu + 1):  # :69-88
+        Se = np.sum(np.abs(np.asarray(E.Sf, np.complex128)) ** 2, axis=3)
+        if C is None or not C.has("Ma"):
+            Se = Se + R.Ti.reshape(Se.shape)
+        Se = (Se + la * p / 2) ** -1
+        Rr = Rr.copy(Sh=Sh.copy(la=la))
+        x, _, _ = CGsolver(y, E, EH, Struct(Se=Se.reshape(x.shape)), C, Rr, x, 3, "None", tol, method, dtype)
+        if n != nOu:
+            Sh = Sh.copy(We=(compute_shearlet(x.reshape(NN), S) + epsil) ** (p - 2))
+            Rr = Rr.copy(Sh=Sh)
+            trReg, _ = trace_estimation(x, None, None, C, Rr, 1e-2, 4, noise)
+            la = (2 / p) * trFid / (trReg + EPS)
+            lam.append(la)
+            Sh = Sh.copy(la=la)
+    return x, np.array(lam + [0.0] * (nOu + 1 - len(lam)))
 
 # Hessian index pairs ha (LMsolver.m:26): 6 diagonal entries then nchoosek(1:6,2)
 HA = [(i, i) for i in range(6)] + list(itertools.combinations(range(6), 2))
