@@ -696,6 +696,65 @@ def io_and_sampling(x, N, shots):
                                      % (N[0], N[1], U, U)}}
 
 
+def cs_arm(ctx, sc, cfg, x, T):
+    """The compressed-sensing reconstruction after the aligned one
+    (Reconstruction/CSsolver.m as solveXT.m:487 calls it when computeCSRecon
+    is set): the shearlet-regularised CG (2 outer x 3 CG iterations, lambda
+    from trace estimates) of the full-size scan with its compressed coils,
+    the estimated motion and unit shot weights, from the aligned image.
+    Timed with CUDA events on the library's stream; the shearlet system's
+    host-side build is timed apart."""
+    import disorder_b200 as db
+    from disorder_b200 import cs, recon
+    N, S = cfg["N"], cfg["shots"]
+    Sc, yc, _, _, _ = db.compressCoils(sc.S, cfg["coils_kept"], sc.y, ctx=ctx)
+    # CSsolver.m's epsil = 1e-2 (:51) is an absolute intensity: the unit-norm
+    # synthetic scan is brought to scanner-like voxel values (about 1e2) first
+    gain = 1e6
+    yc = ctx.upload(yc.numpy() * np.float32(gain))
+    x = ctx.upload(x.numpy() * np.float32(gain))
+    ky, kz, nEc, mSt, _ = recon.level_sampling(sc.H, S, N[:2])
+    cent = [math.ceil((n + 1) / 2.0) for n in N]
+    E = db.Struct(Tr=np.asarray(T, np.float32), NMs=S, NSe=S + 1, Sf=Sc, grids=db.generateTransformGrids(N, N, cent),
+                  ky=ky, kz=kz, nEc=nEc, mSt=mSt)
+    EH = db.Struct(We=np.ones(ky.size, np.float32))
+    R = db.Struct(Ti=np.full(N, 1e-9, np.float32))
+    t0 = time.perf_counter()
+    system = cs.ShearletSystem(ctx, N)
+    t_build = time.perf_counter() - t0
+    rng = np.random.default_rng(1)
+    cs.CSsolver(yc, E, EH, None, None, R, x, tol=1e-3, ctx=ctx, rng=rng, system=system)  # warm-up
+    ctx.synchronize()
+    l0 = ctx.launches
+    ctx.event(0)
+    t0 = time.perf_counter()
+    xc, lam = cs.CSsolver(yc, E, EH, None, None, R, x, tol=1e-3, ctx=ctx, rng=rng, system=system)
+    ctx.event(1)
+    ms = ctx.elapsed_ms(0, 1)
+    wall = time.perf_counter() - t0
+    launches = ctx.launches - l0
+    We = system.coefficients(xc, 1e-2, 1.0)
+    V = int(np.prod(N))
+    reps = 3
+    ctx.event(2)
+    for _ in range(reps):
+        out = system.regularize(xc, We, lam[1])
+    ctx.event(3)
+    ms_reg = ctx.elapsed_ms(2, 3) / reps
+    # a regularizer application makes 6 passes per shearlet + 6, each a read
+    # and a write of the complex volume
+    passes = 6 * system.n_filters + 6
+    res = {"s": ms * 1e-3, "wall_s": wall, "build_s": t_build, "lambda": [float(v) for v in lam],
+           "nrmse": nrmse(ctx, xc, sc.x_gt_host * gain), "nrmse_aligned": nrmse(ctx, x, sc.x_gt_host * gain),
+           "data_gain": gain,
+           "gpu_launches": int(launches), "shearlets": system.n_filters,
+           "regularizer": {"ms": ms_reg, "passes": passes, "GBps": passes * 16.0 * V / (ms_reg * 1e-3) / 1e9},
+           "workload": "CSsolver of the %s scan x %g, %d compressed coils, %d states, 50 3-D shearlets (J=1, 'kos')"
+                       % ("x".join(map(str, N)), gain, Sc.shape[3], S)}
+    del We, out, system, xc, Sc, yc
+    return res
+
+
 # ---------------------------------------------------------------- ranks
 def replica_seed(seed, rank):
     """Each replica reconstructs its own scan: the synthetic seed moves with the rank."""
@@ -737,6 +796,9 @@ def main():
     ap.add_argument("--plain", action="store_true",
                     help="headline = the plain FP32 method (no proposal, no tensor-core passes)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch of uneven scans")
+    ap.add_argument("--no-cs", action="store_true", help="skip the compressed-sensing reconstruction")
+    ap.add_argument("--cs-only", action="store_true",
+                    help="one plain reconstruction, then only the compressed-sensing reconstruction")
     ap.add_argument("--n3", type=int, default=0,
                     help="readout length for --transform-only / --operator-only (a small case for profilers)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16x3", "tf32x3"],
@@ -797,6 +859,10 @@ def main():
     cfg_r = dict(cfg)
     cfg_r["seed"] = replica_seed(cfg["seed"], rank)
     sc = build_scan(ctx, cfg_r)
+    if args.cs_only:
+        x, T, _ = recon.aligned_reconstruction(ctx, sc.S, sc.y, sc.H, cfg["shots"], cfg["N"], perc=cfg["coils_kept"])
+        print(json.dumps({"cs": cs_arm(ctx, sc, cfg, x, T)}), flush=True)
+        return
     net = None
     if not args.plain and os.path.exists(proposal.WEIGHTS):
         net = proposal.MotionNet.load(ctx, proposal.WEIGHTS)
@@ -843,7 +909,7 @@ def main():
             ms = ranks_max(ms, "cuda:%d" % local)
         ev = logs[-1].events
         d = np.asarray(T, float) - np.asarray(sc.T_gt, float)
-        return {"ms": ms, "x": x, "one": one, "clocks": clocks, "launches": int(launches / args.steps),
+        return {"ms": ms, "x": x, "T": T, "one": one, "clocks": clocks, "launches": int(launches / args.steps),
                 "nrmse": nrmse(ctx, x, sc.x_gt_host),
                 "motion_max_err": {"trans_vox": float(np.max(np.abs(d[:, :3]))),
                                    "rot_deg": float(np.degrees(np.max(np.abs(d[:, 3:]))))},
@@ -943,6 +1009,8 @@ def main():
     # baseline, config 1) run at N = 1 only
     if world == 1:
         out["io"] = io_and_sampling(head["x"], cfg["N"], cfg["shots"])
+    if world == 1 and not args.no_cs:
+        out["cs"] = cs_arm(ctx, sc, cfg, plain["x"], plain["T"])
     if world == 1 and not args.no_batch:
         # free the benchmark scan first: the batch holds about 45 GB of scans
         del sc

@@ -108,6 +108,7 @@ SIGNATURES = [
     ("disorder_shearlet_coefficients", C.c_int, [VP, VP, VP, C.c_float, C.c_float, VP]),
     ("disorder_shearlet_regularize", C.c_int, [VP, VP, VP, VP, C.c_float, C.c_float, VP]),
     ("disorder_shearlet_trace", C.c_int, [VP, VP, VP, VP, DP]),
+    ("disorder_trace_probe", C.c_int, [VP, C.c_int64, C.c_uint64, VP, VP]),
     ("disorder_fidelity_trace", C.c_int, [VP, C.POINTER(I32), VP, VP, I32, VP, DP]),
     ("disorder_cg_solve_shearlet", C.c_int, [VP, VP, VP, VP, I32, FP, VP, VP, VP, VP, VP, VP, VP, VP, C.c_float,
                                              VP, I32, I32, I32, C.c_double, DP, C.POINTER(I32),

@@ -99,11 +99,16 @@ def _weight_grid(E, EH):
     return W.astype(np.float32)
 
 
+class _DeviceProbes:
+    """Probes drawn on the device (disorder_trace_probe), seeded from rng."""
+
+    def __init__(self, rng):
+        self.rng = rng if rng is not None else np.random.default_rng()
+
+
 def _noise_source(noise, rng):
-    if noise is not None:
-        return noise
-    rng = rng if rng is not None else np.random.default_rng()
-    return lambda shape: rng.standard_normal(shape).astype(np.float32)
+    """noise(shape) -> host float32 probes (given), else device probes."""
+    return noise if noise is not None else _DeviceProbes(rng)
 
 
 def traceEstimation(ctx, NX, E=None, EH=None, Cs=None, R=None, tol=1e-2, BlSz=1, noise=None, rng=None):
@@ -111,13 +116,16 @@ def traceEstimation(ctx, NX, E=None, EH=None, Cs=None, R=None, tol=1e-2, BlSz=1,
     estimates of the fidelity term (E.Sf with EH.We on the k-space grid) and
     the shearlet term (R.Sh), BlSz real Gaussian probes per round until the
     standard error is below tol of the mean. noise(shape) or rng draws the
-    probes. Returns (tr, trF)."""
+    probes (the device draws them from rng's seeds when noise is None).
+    Returns (tr, trF)."""
     NX = tuple(int(n) for n in NX[:3])
     V = int(np.prod(NX))
-    draw = _noise_source(noise, rng)
-    Ma = None
+    draw = noise if noise is not None else _noise_source(None, rng)
+    Ma = Mad = None
     if Cs is not None and Cs.has("Ma"):
         Ma = _host(Cs.Ma).reshape(NX, order="F").astype(np.float64)
+        Mad = ctx.upload(Ma.astype(np.float32), np.float32)
+    pd = ctx.empty(NX, np.float32)
     Wd = Sd = None
     nC = 0
     if E is not None:
@@ -131,11 +139,16 @@ def traceEstimation(ctx, NX, E=None, EH=None, Cs=None, R=None, tol=1e-2, BlSz=1,
     trF = []
     while True:
         for _ in range(BlSz):
-            v = np.asarray(draw(NX), np.float64)
-            v = v / np.sqrt(np.sum(v * v) / V)  # traceEstimation.m:35
-            if Ma is not None:
-                v = v * Ma
-            pd = ctx.upload(v.astype(np.float32), np.float32)
+            if isinstance(draw, _DeviceProbes):  # traceEstimation.m:34-38 on the device
+                seed = int(draw.rng.integers(1, 2 ** 63))
+                ctx.check(ctx.lib.disorder_trace_probe(ctx.h, V, seed, Mad.ptr if Mad is not None else None, pd.ptr))
+            else:
+                v = np.asarray(draw(NX), np.float64)
+                v = v / np.sqrt(np.sum(v * v) / V)  # traceEstimation.m:35
+                if Ma is not None:
+                    v = v * Ma
+                h = np.asfortranarray(v.astype(np.float32))
+                ctx.check(ctx.lib.disorder_memcpy_h2d(ctx.h, pd.ptr, h.ctypes.data, h.nbytes))
             tc = 0.0
             if E is not None:
                 t = C.c_double()

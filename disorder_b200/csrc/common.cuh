@@ -78,6 +78,23 @@ DIS_HD float2 cfma(float2 a, float2 b, float2 acc) {
   return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y)));
 }
 
+// Counter-based normal variates: the SplitMix64 finaliser of (seed, index)
+// gives two 32-bit uniforms, Box-Muller turns them into two independent
+// standard normals that depend only on (seed, e).
+DIS_D uint64_t dis_mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// (radius, cos, sin) of the pair; the normals are rad * c and rad * s
+DIS_D void dis_normal2_polar(uint64_t seed, long long e, float* rad, float* c, float* s) {
+  const uint64_t r = dis_mix64(seed * 0x9E3779B97F4A7C15ull + (uint64_t)e);
+  const float u1 = ((float)(uint32_t)(r >> 32) + 1.0f) * 2.3283064365386963e-10f;  // (0, 1]
+  const float u2 = (float)(uint32_t)r * 2.3283064365386963e-10f;                   // [0, 1)
+  *rad = sqrtf(-2.0f * logf(u1));
+  sincospif(2.0f * u2, s, c);
+}
+
 // Status plumbing shared by the host-side orchestration code.
 #define DIS_CUDA_TRY(call)                                                   \
   do {                                                                       \

@@ -454,3 +454,59 @@ disorder_ctx_s* dis_shearlet_ctx(const disorder_shearlet_s* sh) { return sh->ctx
 void dis_shearlet_size(const disorder_shearlet_s* sh, int* N) {
   for (int m = 0; m < 3; ++m) N[m] = sh->N[m];
 }
+
+namespace {
+
+// probe[2e], probe[2e+1] = the two normals of (seed, e); sum += their squares
+__global__ void probe_kernel(float* __restrict__ probe, long long V, uint64_t seed, double* __restrict__ sum) {
+  __shared__ double red[kThr / 32];
+  double part = 0.0;
+  const long long n2 = (V + 1) / 2;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n2; e += (long long)gridDim.x * blockDim.x) {
+    float rad, c, s;
+    dis_normal2_polar(seed, e, &rad, &c, &s);
+    const float a = rad * c, b = rad * s;
+    probe[2 * e] = a;
+    part += (double)a * a;
+    if (2 * e + 1 < V) {
+      probe[2 * e + 1] = b;
+      part += (double)b * b;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < kThr / 32; ++w) t += red[w];
+    atomicAdd(sum, t);
+  }
+}
+
+// probe *= (sum / V)^-1/2 (times the mask when given)
+__global__ void probe_scale_kernel(float* __restrict__ probe, long long V, const double* __restrict__ sum,
+                                   const float* __restrict__ mask) {
+  const float s = (float)(1.0 / sqrt(*sum / (double)V));
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < V; i += (long long)gridDim.x * blockDim.x)
+    probe[i] = mask ? probe[i] * s * mask[i] : probe[i] * s;
+}
+
+}  // namespace
+
+int disorder_trace_probe(disorder_ctx ctx, int64_t V, uint64_t seed, const float* mask, float* probe) {
+  if (!ctx) return DISORDER_BAD_ARG;
+  if (!probe || V < 1) return dis_set_error(ctx, DISORDER_BAD_ARG, "trace_probe: bad arguments");
+  DIS_CUDA_TRY(cudaSetDevice(ctx->device));
+  Workspace sw;
+  DIS_TRY(dis_small(ctx, &sw));
+  double* sum = sw.take<double>(1);
+  DIS_CUDA_TRY(cudaMemsetAsync(sum, 0, sizeof(double), ctx->stream));
+  const int blocks = (int)std::min<long long>(((V + 1) / 2 + kThr - 1) / kThr, 8LL * ctx->sm_count);
+  probe_kernel<<<blocks, kThr, 0, ctx->stream>>>(probe, V, seed, sum);
+  dis_count(ctx);
+  const int b2 = (int)std::min<long long>((V + kThr - 1) / kThr, 8LL * ctx->sm_count);
+  probe_scale_kernel<<<b2, kThr, 0, ctx->stream>>>(probe, V, sum, mask);
+  dis_count(ctx);
+  DIS_CUDA_TRY(cudaGetLastError());
+  return DISORDER_OK;
+}

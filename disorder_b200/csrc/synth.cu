@@ -104,22 +104,10 @@ __global__ void scale_kernel(float2* __restrict__ x, long long n, float s) {
     x[e] = cscale(x[e], s);
 }
 
-// SplitMix64 finaliser of (seed, index): a counter-based stream
-DIS_D uint64_t mix64(uint64_t z) {
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-
 __global__ void noise_kernel(float2* __restrict__ y, long long n, float sigma, uint64_t seed) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-    const uint64_t r = mix64(seed * 0x9E3779B97F4A7C15ull + (uint64_t)e);
-    // two uniforms in (0, 1] and [0, 1) from the two 32-bit halves
-    const float u1 = ((float)(uint32_t)(r >> 32) + 1.0f) * 2.3283064365386963e-10f;
-    const float u2 = (float)(uint32_t)r * 2.3283064365386963e-10f;
-    const float rad = sqrtf(-2.0f * logf(u1));
-    float s, c;
-    sincospif(2.0f * u2, &s, &c);
+    float rad, c, s;
+    dis_normal2_polar(seed, e, &rad, &c, &s);
     const float2 v = y[e];
     y[e] = make_float2(v.x + sigma * rad * c, v.y + sigma * rad * s);
   }

@@ -130,3 +130,26 @@ def test_cssolver_against_the_oracle(env):
     assert rel(lam[:2], lamo[:2]) < TOL_SOLVER
     assert rel(x.numpy(), xo) < TOL_SOLVER
     assert np.all(np.isfinite(x.numpy()))
+
+
+def test_device_probes(env):
+    db, cs, osh, ctx, sc, Ed, Eo, sysd, So = env
+    V = int(np.prod(N))
+    a, b = ctx.empty(N, np.float32), ctx.empty(N, np.float32)
+    for d in (a, b):
+        ctx.check(ctx.lib.disorder_trace_probe(ctx.h, V, 1234, None, d.ptr))
+    pa, pb = a.numpy(), b.numpy()
+    assert np.array_equal(pa, pb)  # a function of (seed, index) only
+    assert abs(np.mean(pa.astype(np.float64) ** 2) - 1) < 1e-5  # traceEstimation.m:35
+    assert abs(np.mean(pa)) < 0.02 and 0.9 < np.std(pa) < 1.1
+    mask = (np.random.default_rng(9).uniform(size=N) > 0.5).astype(np.float32)
+    ctx.check(ctx.lib.disorder_trace_probe(ctx.h, V, 1234, ctx.upload(mask).ptr, b.ptr))
+    assert np.allclose(b.numpy(), pa * mask, rtol=1e-6, atol=0)
+    ctx.check(ctx.lib.disorder_trace_probe(ctx.h, V, 99, None, b.ptr))
+    assert not np.allclose(b.numpy(), pa)
+    # with device probes the estimates agree with the host-probe ones to their
+    # statistical spread
+    we = np.ones(sc.ky.size, np.float32)
+    t_dev, _ = cs.traceEstimation(ctx, N, Ed, db.Struct(We=we), None, None, 1e-2, 4, rng=np.random.default_rng(1))
+    t_host, _ = cs.traceEstimation(ctx, N, Ed, db.Struct(We=we), None, None, 1e-2, 4, noise=_probes(3))
+    assert abs(t_dev / t_host - 1) < 0.03
