@@ -696,7 +696,7 @@ def io_and_sampling(x, N, shots):
                                      % (N[0], N[1], U, U)}}
 
 
-def cs_arm(ctx, sc, cfg, x, T):
+def cs_arm(ctx, sc, cfg, x, T, with_cpu=False):
     """The compressed-sensing reconstruction after the aligned one
     (Reconstruction/CSsolver.m as solveXT.m:487 calls it when computeCSRecon
     is set): the shearlet-regularised CG (2 outer x 3 CG iterations, lambda
@@ -741,18 +741,107 @@ def cs_arm(ctx, sc, cfg, x, T):
         out = system.regularize(xc, We, lam[1])
     ctx.event(3)
     ms_reg = ctx.elapsed_ms(2, 3) / reps
-    # a regularizer application makes 6 passes per shearlet + 6, each a read
-    # and a write of the complex volume
-    passes = 6 * system.n_filters + 6
+    # a regularizer application: DFT3 of x (3 passes), per shearlet 5 passes
+    # (inverse along dims 1-2, the dim-3 round trip with We, forward along
+    # dims 2-1 accumulating S .*), the inverse DFT3 of the sum (3 passes).
+    # Algorithmic bytes per voxel: 16 per pass (read + write complex), + 4 for
+    # We on the round trip, + 8 for the accumulator's read on the last pass
+    passes = 5 * system.n_filters + 6
+    bpv = 6 * 16 + system.n_filters * (5 * 16 + 4 + 8)
+    peak, peak_kind = peaks()
+    ach = bpv * V / (ms_reg * 1e-3) / 1e9
     res = {"s": ms * 1e-3, "wall_s": wall, "build_s": t_build, "lambda": [float(v) for v in lam],
            "nrmse": nrmse(ctx, xc, sc.x_gt_host * gain), "nrmse_aligned": nrmse(ctx, x, sc.x_gt_host * gain),
            "data_gain": gain,
            "gpu_launches": int(launches), "shearlets": system.n_filters,
-           "regularizer": {"ms": ms_reg, "passes": passes, "GBps": passes * 16.0 * V / (ms_reg * 1e-3) / 1e9},
+           "regularizer": {"ms": ms_reg, "passes": passes, "bytes_per_voxel": bpv},
+           "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "peak_kind": peak_kind, "bytes_per_launch": float(bpv * V),
+                        "kernel": "sh_pass_kernel chain of one shearlet regularizer application",
+                        "timing": "CUDA events, mean of %d applications" % reps},
            "workload": "CSsolver of the %s scan x %g, %d compressed coils, %d states, 50 3-D shearlets (J=1, 'kos')"
                        % ("x".join(map(str, N)), gain, Sc.shape[3], S)}
     del We, out, system, xc, Sc, yc
+    if with_cpu:
+        res["small"] = cs_small(ctx)
     return res
+
+
+def shearlet_only(cfg, warmup, steps):
+    """The shearlet regularizer alone at the scan's size: a random image, its
+    coefficients, then W + K applications (CUDA events); about 2.7 GB on the
+    device at 256x256x176 (image, 50 coefficient volumes, 3 work volumes)."""
+    import disorder_b200 as db
+    from disorder_b200 import cs
+    N = tuple(cfg["N"])
+    V = int(np.prod(N))
+    ctx = db.Context(0)
+    rng = np.random.default_rng(3)
+    x = ctx.upload((rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64))
+    system = cs.ShearletSystem(ctx, N)
+    We = system.coefficients(x, 1e-2, 1.0)
+    out = ctx.empty(N)
+    for _ in range(warmup):
+        system.regularize(x, We, 0.5, out=out)
+    ctx.synchronize()
+    ctx.event(0)
+    for _ in range(steps):
+        system.regularize(x, We, 0.5, out=out)
+    ctx.event(1)
+    ms = ctx.elapsed_ms(0, 1) / steps
+    bpv = 6 * 16 + system.n_filters * (5 * 16 + 4 + 8)
+    peak, kind = peaks()
+    ach = bpv * V / (ms * 1e-3) / 1e9
+    print(json.dumps({"shearlet_regularizer_ms": ms, "passes": 5 * system.n_filters + 6, "bytes_per_voxel": bpv,
+                      "achieved_GBps": ach, "frac": ach / peak, "peak_kind": kind,
+                      "workload": "%s, %d shearlets" % ("x".join(map(str, N)), system.n_filters)}), flush=True)
+
+
+def cs_small(ctx):
+    """CSsolver on the 40x36x36 test scan (4 coils, 8 states) on the GPU and
+    by the FP64 oracle in full, from the same image with the same trace
+    probes: both times measured, and the difference of the results."""
+    import disorder_b200 as db
+    from disorder_b200 import cs
+    from disorder_b200 import synth
+    from oracle import encoding as oenc
+    from oracle import solvers as osol
+    from oracle.grids import generateTransformGrids as ogrids
+    N = (40, 36, 36)
+    sc = synth.make_scan(N, 4, 8, 3.0, 2.0, 30.0, 6, 17, np.complex128)
+    cent = [np.ceil((n + 1) / 2.0) for n in N]
+    Eo = oenc.Struct(Tr=sc.T_gt, NMs=8, NSe=9, Sf=sc.S, ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt,
+                     grids=ogrids(N, N, cent, sh=1))
+    Ed = db.Struct(Tr=Eo.Tr, NMs=Eo.NMs, NSe=Eo.NSe, Sf=ctx.upload(sc.S.astype(np.complex64)),
+                   grids=db.generateTransformGrids(N, N, cent, sh=1), ky=sc.ky, kz=sc.kz, nEc=sc.nEc, mSt=sc.mSt)
+    y = oenc.encode(sc.x_gt.astype(np.complex128), Eo) * 1e6
+    x0 = sc.x_gt * 0.9e6
+    Ti = np.full(N, 1e-9)
+    we = np.ones(y.shape[0])
+
+    def probes():
+        r = np.random.default_rng(1)
+        return lambda shape: r.standard_normal(shape).astype(np.float32)
+
+    system = cs.ShearletSystem(ctx, N)
+    cs.CSsolver(y.astype(np.complex64), Ed, db.Struct(We=we.astype(np.float32)), None, None,
+                db.Struct(Ti=Ti.astype(np.float32)), x0.astype(np.complex64), tol=1e-5, ctx=ctx, noise=probes(),
+                system=system)  # warm-up
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    xg, lam = cs.CSsolver(y.astype(np.complex64), Ed, db.Struct(We=we.astype(np.float32)), None, None,
+                          db.Struct(Ti=Ti.astype(np.float32)), x0.astype(np.complex64), tol=1e-5, ctx=ctx,
+                          noise=probes(), system=system)
+    xh = xg.numpy()
+    t_gpu = time.perf_counter() - t0
+    O = Eo.__class__
+    t0 = time.perf_counter()
+    xo, lamo = osol.CSsolver(y, Eo, O(We=we), None, None, O(Ti=Ti), x0, tol=1e-5, noise=probes())
+    t_cpu = time.perf_counter() - t0
+    return {"gpu_s": t_gpu, "oracle_s": t_cpu, "oracle_threads": 1,
+            "rel_err": float(np.linalg.norm(xh - xo) / np.linalg.norm(xo)),
+            "lambda_rel_err": float(np.linalg.norm(lam[:2] - lamo[:2]) / np.linalg.norm(lamo[:2])),
+            "workload": "CSsolver of a 40x36x36 scan, 4 coils, 8 states, host probes, wall times"}
 
 
 # ---------------------------------------------------------------- ranks
@@ -797,6 +886,7 @@ def main():
                     help="headline = the plain FP32 method (no proposal, no tensor-core passes)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch of uneven scans")
     ap.add_argument("--no-cs", action="store_true", help="skip the compressed-sensing reconstruction")
+    ap.add_argument("--shearlet-only", action="store_true", help="only time the shearlet regularizer")
     ap.add_argument("--cs-only", action="store_true",
                     help="one plain reconstruction, then only the compressed-sensing reconstruction")
     ap.add_argument("--n3", type=int, default=0,
@@ -816,6 +906,8 @@ def main():
         return transform_only(cfg, args.transform_only, args.warmup, args.steps, args.precision)
     if args.operator_only:
         return operator_only(cfg, args.operator_only, args.warmup, args.steps, args.profile_region, args.precision)
+    if args.shearlet_only:
+        return shearlet_only(cfg, args.warmup, args.steps)
     if args.batch_only:
         os.environ.setdefault("DISORDER_WORKSPACE_GB", "12")
         print(json.dumps({"batch": batch_arm()}))
@@ -861,7 +953,7 @@ def main():
     sc = build_scan(ctx, cfg_r)
     if args.cs_only:
         x, T, _ = recon.aligned_reconstruction(ctx, sc.S, sc.y, sc.H, cfg["shots"], cfg["N"], perc=cfg["coils_kept"])
-        print(json.dumps({"cs": cs_arm(ctx, sc, cfg, x, T)}), flush=True)
+        print(json.dumps({"cs": cs_arm(ctx, sc, cfg, x, T, with_cpu=not args.no_cpu)}), flush=True)
         return
     net = None
     if not args.plain and os.path.exists(proposal.WEIGHTS):
@@ -1010,7 +1102,7 @@ def main():
     if world == 1:
         out["io"] = io_and_sampling(head["x"], cfg["N"], cfg["shots"])
     if world == 1 and not args.no_cs:
-        out["cs"] = cs_arm(ctx, sc, cfg, plain["x"], plain["T"])
+        out["cs"] = cs_arm(ctx, sc, cfg, plain["x"], plain["T"], with_cpu=not args.no_cpu)
     if world == 1 and not args.no_batch:
         # free the benchmark scan first: the batch holds about 45 GB of scans
         del sc

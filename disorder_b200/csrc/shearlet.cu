@@ -21,73 +21,12 @@
 #include <cmath>
 #include <vector>
 
-#include "fft.cuh"
-#include "internal.h"
-#include "tiles.cuh"
-
-struct disorder_shearlet_s {
-  disorder_ctx_s* ctx = nullptr;
-  int N[3] = {0, 0, 0};
-  int n_planes = 0;
-  int n_filters = 0;
-  float2* planes = nullptr;   // pair blocks, each n_planes planes of Na x Nb (column-major)
-  long long pair_off[3] = {0, 0, 0};
-  long long plane_size[3] = {0, 0, 0};
-  std::vector<int> table;     // n_filters x 4: pair A, plane A, pair B, plane B
-};
+#include "fastpass.h"
+#include "shearlet.cuh"
 
 namespace {
 
-constexpr int kThr = 256;
-// the dimension pairs of the 2-D planes (0-based), first dimension fastest
-constexpr int kPair[3][2] = {{0, 1}, {0, 2}, {2, 1}};
-
-enum { PRE_NONE = 0, PRE_CONJ_FILTER = 1, PRE_COIL = 2 };
-enum {
-  POST_STORE = 0,       // out = v
-  POST_TIMES_WE = 1,    // out = We .* v
-  POST_COEF = 2,        // we_out = (|v| + eps)^pw
-  POST_ACC_FILTER = 3,  // acc += S_w .* v
-  POST_TRACE_WE = 4,    // sum += We |v|^2
-  POST_TRACE_GRID = 5,  // sum += scale W(k1, k2) |v|^2
-  POST_AXPBY = 6        // out = beta out + scale v
-};
-
-struct ShFilt {
-  const float2* A = nullptr;
-  const float2* B = nullptr;
-  int pa = 0, pb = 0;
-};
-
-struct ShArgs {
-  int N[3];
-  int axis = 0;
-  int inv = 0;  // inverse DFT (1/n scaled)
-  FFTPlan plan;
-  int L = 16, P = 17;
-  const float2* in = nullptr;
-  const float* in_real = nullptr;  // real input instead of `in`
-  float2* out = nullptr;
-  int pre = PRE_NONE;
-  const float2* pre_c = nullptr;
-  int post = POST_STORE;
-  const float* we = nullptr;
-  float* we_out = nullptr;
-  float eps = 0.f, pw = -1.f;
-  float2* acc = nullptr;
-  const float* wgrid = nullptr;
-  float beta = 0.f, scale = 1.f;
-  ShFilt f;
-  double* sum = nullptr;
-};
-
-DIS_D int pair_index(int q, int c0, int c1, int c2, const int* N) {
-  return q == 0 ? c0 + N[0] * c1 : (q == 1 ? c0 + N[0] * c2 : c2 + N[2] * c1);
-}
-
-DIS_D float2 filter_at(const ShFilt& f, int c0, int c1, int c2, const int* N) {
-  return cmul(f.A[pair_index(f.pa, c0, c1, c2, N)], f.B[pair_index(f.pb, c0, c1, c2, N)]);
-}
+using namespace shl;
 
 __global__ void __launch_bounds__(kThr) sh_pass_kernel(ShArgs a) {
   extern __shared__ float2 sm[];
@@ -130,10 +69,20 @@ __global__ void __launch_bounds__(kThr) sh_pass_kernel(ShArgs a) {
   __syncthreads();
   const float2* X = fft_tile(b0, b1, tw, a.plan, L, P, tid, nthr);
   const float invn = 1.0f / (float)n;
+  bool inv = a.inv;
+  if (a.mid_we) {
+    // X holds conj(n IDFT(v)); the forward DFT's input is IDFT(v) .* We
+    float2* Xw = const_cast<float2*>(X);
+    for_tile(tl, a.N, axis, n, L, P, tid, nthr,
+             [&](long long g, int s) { Xw[s] = cscale(cconj(Xw[s]), invn * a.mid_we[g]); });
+    __syncthreads();
+    X = fft_tile(Xw, Xw == b0 ? b1 : b0, tw, a.plan, L, P, tid, nthr);
+    inv = false;
+  }
   double part = 0.0;
   for_tile(tl, a.N, axis, n, L, P, tid, nthr, [&](long long g, int s) {
     float2 v = X[s];
-    if (a.inv) v = cscale(cconj(v), invn);
+    if (inv) v = cscale(cconj(v), invn);
     switch (a.post) {
       case POST_STORE: a.out[g] = v; break;
       case POST_TIMES_WE: a.out[g] = cscale(v, a.we[g]); break;
@@ -176,6 +125,12 @@ __global__ void __launch_bounds__(kThr) sh_pass_kernel(ShArgs a) {
 
 int sh_pass(disorder_ctx_s* ctx, ShArgs a) {
   const int n = a.N[a.axis];
+  const int kind = fast_kind(a);
+  if (dis_use_fast() && kind >= 0 && (sh_fast_a(ctx, a, kind) || sh_fast_b(ctx, a, kind))) {
+    dis_count(ctx);
+    DIS_CUDA_TRY(cudaGetLastError());
+    return DISORDER_OK;
+  }
   if (!dis_make_fft_plan(n, &a.plan))
     return dis_set_error(ctx, DISORDER_UNSUPPORTED_FIELD, "shearlet: length %d has a prime factor above 13", n);
   a.L = 16;
@@ -353,15 +308,17 @@ int dis_shearlet_regularize(disorder_ctx_s* ctx, const disorder_shearlet_s* sh, 
   DIS_TRY(dft3(ctx, sh->N, x, nullptr, xF));
   DIS_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(float2) * V, ctx->stream));
   for (int w = 0; w < sh->n_filters; ++w) {
-    ShArgs last = base(sh->N, 2, 1);
-    last.post = POST_TIMES_WE;
-    last.we = We + (long long)w * V;
-    DIS_TRY(filtered_inverse(ctx, sh, w, xF, t, last));
-    for (int m = 0; m < 3; ++m) {
+    // inverse along dims 1-2 (conj(S_w) on the first load); along dim 3 the
+    // inverse, We_w and the forward DFT in one pass; forward along dims 2, 1
+    // with S_w .* accumulated on the last store: 5 passes per shearlet
+    ShArgs mid = base(sh->N, 2, 1);
+    mid.mid_we = We + (long long)w * V;
+    DIS_TRY(filtered_inverse(ctx, sh, w, xF, t, mid));
+    for (int m = 1; m >= 0; --m) {
       ShArgs a = base(sh->N, m, 0);
       a.in = t;
       a.out = t;
-      if (m == 2) {
+      if (m == 0) {
         a.post = POST_ACC_FILTER;
         a.acc = acc;
         a.f = filt(sh, w);

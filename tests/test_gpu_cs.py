@@ -153,3 +153,30 @@ def test_device_probes(env):
     t_dev, _ = cs.traceEstimation(ctx, N, Ed, db.Struct(We=we), None, None, 1e-2, 4, rng=np.random.default_rng(1))
     t_host, _ = cs.traceEstimation(ctx, N, Ed, db.Struct(We=we), None, None, 1e-2, 4, noise=_probes(3))
     assert abs(t_dev / t_host - 1) < 0.03
+
+
+@pytest.mark.parametrize("Nf", [(64, 64, 44), (64, 96, 88)])
+def test_register_fft_passes(Nf):
+    """Lengths with a fast factorisation take the register-FFT pass kernel
+    (64 = 8 x 8, 44 = 4 x 11, 96 = 8 x 12, 88 = 8 x 11; the
+    generic kernel covers the 40 and 36 of the other tests)."""
+    import disorder_b200 as db
+    from disorder_b200 import cs
+    from oracle import shearlet as osh
+    ctx = db.Context(0)
+    rng = np.random.default_rng(12)
+    x = (rng.standard_normal(Nf) + 1j * rng.standard_normal(Nf)).astype(np.complex64)
+    u = (rng.standard_normal(Nf) + 1j * rng.standard_normal(Nf)).astype(np.complex64)
+    sysd = cs.ShearletSystem(ctx, Nf)
+    So = osh.buildShearlet(list(Nf), 1, [1])["S"]
+    We = sysd.coefficients(ctx.upload(x), 1e-2, 1.0)
+    Weo = (osh.compute_shearlet(x.astype(np.complex128), So) + 1e-2) ** -1.0
+    assert rel(We.numpy(), Weo) < TOL
+    Wh = We.numpy().astype(np.float64)
+    r = sysd.regularize(ctx.upload(u), We, 0.3)
+    assert rel(r.numpy(), osh.regularize_sh(u.astype(np.complex128), So, Wh, 0.3)) < TOL
+    probe = rng.standard_normal(Nf).astype(np.float32)
+    t = sysd.trace(ctx.upload(probe), We)
+    pF = np.fft.fftn(probe.astype(np.complex128))
+    to = sum(float(np.sum(Wh[..., w] * np.abs(np.fft.ifftn(np.conj(So[..., w]) * pF)) ** 2)) for w in range(So.shape[-1]))
+    assert abs(t / to - 1) < TOL
