@@ -159,6 +159,13 @@ ShArgs base(const int* N, int axis, int inv) {
   return a;
 }
 
+// a pass of a shearlet operator: the system's grid and twiddle table
+ShArgs base(const disorder_shearlet_s* sh, int axis, int inv) {
+  ShArgs a = base(sh->N, axis, inv);
+  a.twg = sh->tw[axis];
+  return a;
+}
+
 ShFilt filt(const disorder_shearlet_s* sh, int w) {
   const int* t = &sh->table[4 * w];
   ShFilt f;
@@ -171,9 +178,9 @@ ShFilt filt(const disorder_shearlet_s* sh, int w) {
 
 // out = DFT3(x) (x complex, or real when xr is given); with PRE_COIL the
 // first pass multiplies by the coil map c.
-int dft3(disorder_ctx_s* ctx, const int* N, const float2* x, const float* xr, float2* out) {
+int dft3(disorder_ctx_s* ctx, const disorder_shearlet_s* sh, const float2* x, const float* xr, float2* out) {
   for (int m = 0; m < 3; ++m) {
-    ShArgs a = base(N, m, 0);
+    ShArgs a = base(sh, m, 0);
     a.in = m == 0 ? x : out;
     a.in_real = m == 0 ? xr : nullptr;
     a.out = out;
@@ -186,7 +193,7 @@ int dft3(disorder_ctx_s* ctx, const int* N, const float2* x, const float* xr, fl
 int filtered_inverse(disorder_ctx_s* ctx, const disorder_shearlet_s* sh, int w, const float2* xF, float2* t,
                      const ShArgs& last) {
   for (int m = 0; m < 3; ++m) {
-    ShArgs a = m == 2 ? last : base(sh->N, m, 1);
+    ShArgs a = m == 2 ? last : base(sh, m, 1);
     a.axis = m;
     a.inv = 1;
     a.in = m == 0 ? xF : t;
@@ -252,12 +259,28 @@ int disorder_shearlet_create(disorder_ctx ctx, const int32_t N[3], int32_t n_pla
     delete sh;
     return dis_set_error(ctx, DISORDER_OOM, "shearlet_create: planes");
   }
+  for (int m = 0; m < 3; ++m) {
+    std::vector<float2> w(N[m]);
+    for (int k = 0; k < N[m]; ++k) {
+      const double ang = -2.0 * 3.14159265358979323846 * (double)k / (double)N[m];
+      w[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+    if (cudaMalloc(&sh->tw[m], sizeof(float2) * N[m]) != cudaSuccess ||
+        cudaMemcpy(sh->tw[m], w.data(), sizeof(float2) * N[m], cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      for (int q = 0; q <= m; ++q) cudaFree(sh->tw[q]);
+      cudaFree(sh->planes);
+      delete sh;
+      return dis_set_error(ctx, DISORDER_OOM, "shearlet_create: twiddle tables");
+    }
+  }
   const void* src[3] = {planes0, planes1, planes2};
   for (int q = 0; q < 3; ++q) {
     const cudaError_t e = cudaMemcpy(sh->planes + sh->pair_off[q], src[q], sizeof(float2) * sh->plane_size[q] * n_planes,
                                      cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
       cudaFree(sh->planes);
+      for (int m = 0; m < 3; ++m) cudaFree(sh->tw[m]);
       delete sh;
       return dis_set_error(ctx, DISORDER_CUDA_ERR, "shearlet_create: %s", cudaGetErrorString(e));
     }
@@ -271,6 +294,7 @@ int disorder_shearlet_destroy(disorder_shearlet sh) {
   cudaSetDevice(sh->ctx->device);
   cudaStreamSynchronize(sh->ctx->stream);
   cudaFree(sh->planes);
+  for (int m = 0; m < 3; ++m) cudaFree(sh->tw[m]);
   delete sh;
   return DISORDER_OK;
 }
@@ -284,9 +308,9 @@ int disorder_shearlet_coefficients(disorder_ctx ctx, disorder_shearlet sh, const
   DIS_TRY(dis_workspace(ctx, sizeof(float2) * 2 * V + 1024, &ws));
   float2* xF = ws.take<float2>(V);
   float2* t = ws.take<float2>(V);
-  DIS_TRY(dft3(ctx, sh->N, (const float2*)x, nullptr, xF));
+  DIS_TRY(dft3(ctx, sh, (const float2*)x, nullptr, xF));
   for (int w = 0; w < sh->n_filters; ++w) {
-    ShArgs last = base(sh->N, 2, 1);
+    ShArgs last = base(sh, 2, 1);
     last.post = POST_COEF;
     last.we_out = We + (long long)w * V;
     last.eps = eps;
@@ -305,17 +329,17 @@ int dis_shearlet_regularize(disorder_ctx_s* ctx, const disorder_shearlet_s* sh, 
   float2* xF = ws.take<float2>(V);
   float2* t = ws.take<float2>(V);
   float2* acc = ws.take<float2>(V);
-  DIS_TRY(dft3(ctx, sh->N, x, nullptr, xF));
+  DIS_TRY(dft3(ctx, sh, x, nullptr, xF));
   DIS_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(float2) * V, ctx->stream));
   for (int w = 0; w < sh->n_filters; ++w) {
     // inverse along dims 1-2 (conj(S_w) on the first load); along dim 3 the
     // inverse, We_w and the forward DFT in one pass; forward along dims 2, 1
     // with S_w .* accumulated on the last store: 5 passes per shearlet
-    ShArgs mid = base(sh->N, 2, 1);
+    ShArgs mid = base(sh, 2, 1);
     mid.mid_we = We + (long long)w * V;
     DIS_TRY(filtered_inverse(ctx, sh, w, xF, t, mid));
     for (int m = 1; m >= 0; --m) {
-      ShArgs a = base(sh->N, m, 0);
+      ShArgs a = base(sh, m, 0);
       a.in = t;
       a.out = t;
       if (m == 0) {
@@ -327,7 +351,7 @@ int dis_shearlet_regularize(disorder_ctx_s* ctx, const disorder_shearlet_s* sh, 
     }
   }
   for (int m = 0; m < 3; ++m) {
-    ShArgs a = base(sh->N, m, 1);
+    ShArgs a = base(sh, m, 1);
     a.in = acc;
     a.out = m == 2 ? out : acc;
     if (m == 2) {
@@ -358,9 +382,9 @@ int disorder_shearlet_trace(disorder_ctx ctx, disorder_shearlet sh, const float*
   float2* t = ws.take<float2>(V);
   double* sum = sw.take<double>(1);
   DIS_CUDA_TRY(cudaMemsetAsync(sum, 0, sizeof(double), ctx->stream));
-  DIS_TRY(dft3(ctx, sh->N, nullptr, probe, xF));
+  DIS_TRY(dft3(ctx, sh, nullptr, probe, xF));
   for (int w = 0; w < sh->n_filters; ++w) {
-    ShArgs last = base(sh->N, 2, 1);
+    ShArgs last = base(sh, 2, 1);
     last.post = POST_TRACE_WE;
     last.we = We + (long long)w * V;
     last.sum = sum;

@@ -18,6 +18,7 @@ struct disorder_shearlet_s {
   long long pair_off[3] = {0, 0, 0};
   long long plane_size[3] = {0, 0, 0};
   std::vector<int> table;     // n_filters x 4: pair A, plane A, pair B, plane B
+  float2* tw[3] = {nullptr, nullptr, nullptr};  // W_N^m of each axis length (device)
 };
 
 namespace shl {
@@ -67,6 +68,7 @@ struct ShArgs {
   float beta = 0.f, scale = 1.f;
   ShFilt f;
   double* sum = nullptr;
+  const float2* twg = nullptr;  // device W_N^m of the axis length (register-FFT kernel), or null
 };
 
 DIS_D int pair_index(int q, int c0, int c1, int c2, const int* N) {
@@ -129,13 +131,17 @@ __global__ void __launch_bounds__(kThr) sh_fast_kernel(ShArgs a) {
   float2* tws = twf + ((N + 1) & ~1);        // the line FFT's twiddles
   float2* exa = tws + ((LN::TWS + 1) & ~1);  // LPB exchange tiles
   const int tid = threadIdx.x, lt = tid % TL, li = tid / TL;
-  for (int m = tid; m < N; m += kThr) {
-    double sn, cs;
-    sincospi(-2.0 * (double)m / (double)N, &sn, &cs);
-    twf[m] = make_float2((float)cs, (float)sn);
+  if (a.twg) {
+    ff::load_tw<F1, F2>(tws, a.twg, tid, kThr);
+  } else {
+    for (int m = tid; m < N; m += kThr) {
+      double sn, cs;
+      sincospi(-2.0 * (double)m / (double)N, &sn, &cs);
+      twf[m] = make_float2((float)cs, (float)sn);
+    }
+    __syncthreads();
+    ff::load_tw<F1, F2>(tws, twf, tid, kThr);
   }
-  __syncthreads();
-  ff::load_tw<F1, F2>(tws, twf, tid, kThr);
   __syncthreads();
   float2* ex = exa + li * LN::EXSZ;
   const int axis = a.axis;
