@@ -74,3 +74,61 @@ def test_oracle_regularizer_is_hermitian_positive(systems):
     Rz = osh.regularize_sh(z, o["S"], We, 0.8)
     assert abs(np.vdot(z, Rx) - np.conj(np.vdot(x, Rz))) < 1e-9 * abs(np.vdot(x, Rx))
     assert np.vdot(x, Rx).real > 0 and abs(np.vdot(x, Rx).imag) < 1e-9 * np.vdot(x, Rx).real
+
+
+def test_oracle_trace_estimates_match_the_exact_traces():
+    """traceEstimation.m estimates traces with Gaussian probes; both of its
+    operators have closed-form traces to check the oracle against:
+    - shearlet term: A_w = IDFT diag(conj S_w) DFT is circulant, so every row
+      has squared norm mean_k |S_w(k)|^2 and tr = sum_w sum_v We_w(v) mean|S_w|^2;
+    - fidelity term: F the unitary 2-D DFT, tr = mean_k W(k) sum_c sum_v |S_c(v)|^2."""
+    from oracle.encoding import Struct
+    Nt = (36, 36, 36)
+    rng = np.random.default_rng(8)
+    S = osh.buildShearlet(list(Nt), 1, [1])["S"]
+    We = rng.uniform(0.2, 2.0, Nt + (S.shape[-1],))
+    exact = float(np.sum(We.reshape(-1, We.shape[-1]).sum(0) * np.mean(np.abs(S.reshape(-1, S.shape[-1])) ** 2, 0)))
+    pr = np.random.default_rng(9)
+    draw = lambda shape: pr.standard_normal(shape)  # noqa: E731
+    tr, trF = osh.trace_estimation(np.zeros(Nt), None, None, None, Struct(Sh=Struct(S=S, We=We)), 2e-3, 4, draw)
+    se = np.std(trF, ddof=1) / np.sqrt(len(trF))
+    assert abs(tr - exact) < 5 * se + 1e-3 * exact, (tr, exact, se)
+    # fidelity term with coil maps and a weight grid over (ky, kz)
+    Sf = rng.standard_normal(Nt + (3,)) + 1j * rng.standard_normal(Nt + (3,))
+    ky, kz = np.meshgrid(np.arange(Nt[0]), np.arange(Nt[1]), indexing="ij")
+    w = rng.uniform(0.0, 1.5, ky.size)
+    E = Struct(Sf=Sf, ky=ky.ravel(), kz=kz.ravel())
+    exact = float(np.mean(w) * np.sum(np.abs(Sf) ** 2))
+    tr, trF = osh.trace_estimation(np.zeros(Nt), E, Struct(We=w), None, None, 2e-3, 4, draw)
+    se = np.std(trF, ddof=1) / np.sqrt(len(trF))
+    assert abs(tr - exact) < 5 * se + 1e-3 * exact, (tr, exact, se)
+
+
+def test_oracle_cs_beats_cg_at_scanner_intensities():
+    """CSsolver.m's epsil = 0.01 is an absolute intensity: with the unit-norm
+    synthetic image scaled to scanner-like values (x 1e6), the shearlet
+    reconstruction of a noisy scan improves on plain CG; at unit norm it
+    over-smooths."""
+    from conftest import make_problem
+    from oracle import encoding as oenc
+    from oracle import solvers as osol
+    Nt = (40, 36, 36)
+    sc, Eo = make_problem(N=Nt, C=4, S=8, seed=17, dtype=np.complex128, zero_motion=True)
+    O = Eo.__class__
+    rng = np.random.default_rng(6)
+    y0 = oenc.encode(sc.x_gt.astype(np.complex128), Eo)
+    y0 = y0 + 0.05 * np.linalg.norm(y0) / np.sqrt(y0.size) * (rng.standard_normal(y0.shape)
+                                                                 + 1j * rng.standard_normal(y0.shape))
+    Se = 1 / (np.sum(np.abs(sc.S) ** 2, axis=3) + 1e-9)
+    errs = {}
+    for gain in (1.0, 1e6):
+        y = y0 * gain
+        x0, _, _ = osol.CGsolver(y, Eo, O(We=np.ones(y.shape[0])), O(Se=Se), None, None, None, 10, "Energy", 1e-3)
+        pr = np.random.default_rng(1)
+        xc, lam = osol.CSsolver(y, Eo, O(We=np.ones(y.shape[0])), None, None, O(Ti=np.full(Nt, 1e-9)), x0, tol=1e-5,
+                                noise=lambda shape: pr.standard_normal(shape))
+        g = sc.x_gt * gain
+        e = lambda a: float(np.linalg.norm(a.reshape(Nt) - g) / np.linalg.norm(g))  # noqa: E731
+        errs[gain] = (e(x0), e(xc))
+    assert errs[1e6][1] < 0.9 * errs[1e6][0], errs
+    assert errs[1.0][1] > 2 * errs[1.0][0], errs
