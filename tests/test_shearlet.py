@@ -132,3 +132,18 @@ def test_oracle_cs_beats_cg_at_scanner_intensities():
         errs[gain] = (e(x0), e(xc))
     assert errs[1e6][1] < 0.9 * errs[1e6][0], errs
     assert errs[1.0][1] > 2 * errs[1.0][0], errs
+
+
+def test_two_scale_planes_agree():
+    """Two scales with shear levels 1 and 2 (the recursion of the lowpass and
+    highpass filters, buildWedgeBandpassAndLowpassFilters.m:24-30, and two
+    wedge sets) give the same 2-D planes from the device-form builder and the
+    oracle."""
+    Nt = (80, 76, 74)
+    K = [1, 2]
+    o_planes = osh.shearlet_planes(list(Nt), K)
+    d_planes, table, idxs = sh.build_planes(Nt, 2, K)
+    assert len(idxs) == len(osh.shearlet_idxs(3, K, 0)) and table.shape == (len(idxs), 4)
+    for P, Q in zip(d_planes, o_planes):
+        assert P.shape == Q.shape
+        assert np.linalg.norm(P - Q) / np.linalg.norm(Q) < 1e-6
