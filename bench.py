@@ -15,9 +15,13 @@ BF16x3 tensor-core DFT passes and Gram, as the metric names; the plain FP32
 method runs the same way beside it (`plain`, whose NRMSE is the target), each
 half alone once (`learned`, `mixed`), the headline from host arrays (`e2e`),
 the normal operator's roofline, the per-stage error against the FP64 oracle,
-and at N = 1 the data formats either side of the path (`io`), the batch of
-uneven scans (`batch`), the CPU baseline and the small case run in full on
-both (`config1`). `--plain` makes the plain method the headline.
+and at N = 1 the data formats either side of the path (`io`), the
+compressed-sensing reconstruction after the aligned one (`cs`: CSsolver with
+the shearlet regularizer, its roofline, and a small case on the GPU and the
+FP64 oracle), the batch of uneven scans (`batch`), the CPU baseline and the
+small case run in full on both (`config1`). `--plain` makes the plain method
+the headline; `--cs-only` and `--shearlet-only` run only the CS leg or only
+the shearlet regularizer.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 For N > 1 (one process per GPU under torchrun) each GPU reconstructs its own
