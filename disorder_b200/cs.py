@@ -13,7 +13,7 @@ Differences from the reference, all on paths this module does not take:
 - checkFilterFeasibility's fallback filter configurations 2-7 are not built
   (grids below 33 voxels along a dimension raise);
 - the trace estimate's weight grid is zero where no sample falls
-  (traceEstimation.m:24-29 keeps whatever EH.We held there).
+  (traceEstimation.m:42-49 keeps whatever EH.We held there).
 """
 
 import ctypes as C
@@ -81,7 +81,7 @@ class ShearletSystem:
         return out
 
     def trace(self, probe, We):
-        """traceEstimation.m:62-80 for one real probe (device float32 V)."""
+        """traceEstimation.m:85-102 for one real probe (device float32 V)."""
         tr = C.c_double()
         self.ctx.check(self.ctx.lib.disorder_shearlet_trace(self.ctx.h, self.h, probe.ptr, We.ptr, C.byref(tr)))
         return float(tr.value)
@@ -92,7 +92,7 @@ def _host(a):
 
 
 def _weight_grid(E, EH):
-    """EH.We (per sample) on the (ky, kz) grid (traceEstimation.m:24-29)."""
+    """EH.We (per sample) on the (ky, kz) grid (traceEstimation.m:42-49)."""
     N1, N2 = E.Sf.shape[0], E.Sf.shape[1]
     W = np.zeros((N1, N2), np.float64)
     np.add.at(W, (_host(E.ky).ravel(), _host(E.kz).ravel()), _host(EH.We).astype(np.float64).ravel())
@@ -139,12 +139,12 @@ def traceEstimation(ctx, NX, E=None, EH=None, Cs=None, R=None, tol=1e-2, BlSz=1,
     trF = []
     while True:
         for _ in range(BlSz):
-            if isinstance(draw, _DeviceProbes):  # traceEstimation.m:34-38 on the device
+            if isinstance(draw, _DeviceProbes):  # traceEstimation.m:54-59 on the device
                 seed = int(draw.rng.integers(1, 2 ** 63))
                 ctx.check(ctx.lib.disorder_trace_probe(ctx.h, V, seed, Mad.ptr if Mad is not None else None, pd.ptr))
             else:
                 v = np.asarray(draw(NX), np.float64)
-                v = v / np.sqrt(np.sum(v * v) / V)  # traceEstimation.m:35
+                v = v / np.sqrt(np.sum(v * v) / V)  # traceEstimation.m:55
                 if Ma is not None:
                     v = v * Ma
                 h = np.asfortranarray(v.astype(np.float32))

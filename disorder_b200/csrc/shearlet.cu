@@ -1,7 +1,7 @@
 // The shearlet regularizer of the compressed-sensing reconstruction on the
 // device: computeShearlet (Reconstruction/CSsolver.m:91-101), the shearlet
 // branch of Reconstruction/regularize.m:27-46 and the two trace estimates of
-// Reconstruction/traceEstimation.m:40-80.
+// Reconstruction/traceEstimation.m:61-102.
 //
 // A 3-D shearlet of the system built by Shearlets/buildShearlet.m is the
 // product of two 2-D shearlets over different dimension pairs

@@ -12,10 +12,10 @@ Supported: 3-D grids, complex = 0, the filters CSsolver uses ('kos' or 'ko'
 directional filter, 'maxflat2' scaling filter) and checkFilterFeasibility's
 first configuration (every dimension at least 33 for J = 1, K = [1]). The
 pieces follow:
-- getShearletIdxs.m:27-52 (index tables);
+- getShearletIdxs.m:29-74 (index tables);
 - buildDirectionalFilter.m:34-47,149 and buildQuadratureMirrorFilter.m;
-- checkFilterFeasibility.m:4-28;
-- buildWedgeBandpassAndLowpassFilters.m:4-63, with Methods/shearing.m's
+- checkFilterFeasibility.m:16-38;
+- buildWedgeBandpassAndLowpassFilters.m:34-119, with Methods/shearing.m's
   integer shears done as exact circular row shifts (the DFT phase ramp of
   shifting.m:38-47 shifts by exactly that many samples).
 The construction runs once per reconstruction grid, in float64, and the
@@ -119,7 +119,7 @@ def scaling_filter(name="maxflat2"):
 
 
 def feasible(Nab, K, DF, SF):
-    """checkFilterFeasibility.m:4-28, first configuration: True when the
+    """checkFilterFeasibility.m:16-38, first configuration: True when the
     requested filters fit a plane of size Nab."""
     L = SF.size
     l1 = L
@@ -133,7 +133,7 @@ def feasible(Nab, K, DF, SF):
 
 
 def _filters_2d(Nab, K, DF, SF):
-    """buildWedgeBandpassAndLowpassFilters.m:4-63 for one plane orientation:
+    """buildWedgeBandpassAndLowpassFilters.m:34-119 for one plane orientation:
     (wedges {k: (Na, Nb, 2^(k+1)+1)}, bandpass (Na, Nb, J), lowpass)."""
     Na, Nb = Nab
     J, Kmax = len(K), max(K) + 1
@@ -172,7 +172,7 @@ def _filters_2d(Nab, K, DF, SF):
 
 
 def shearlet_idxs(nd, K, full):
-    """getShearletIdxs.m:27-52 (complex = 0): 1-based rows, lowpass last."""
+    """getShearletIdxs.m:29-74 (complex = 0): 1-based rows, lowpass last."""
     rows = []
     if nd == 2:
         for cone in (1, 2):

@@ -426,15 +426,15 @@ int disorder_shearlet_coefficients(disorder_ctx ctx, disorder_shearlet sh, const
  * scale = R.Sh.la*R.Sh.p/2. x, out: device V complex (out may not alias x). */
 int disorder_shearlet_regularize(disorder_ctx ctx, disorder_shearlet sh, const void* x, const float* We,
                                  float scale, float beta, void* out);
-/* Regularizer term of traceEstimation.m:62-80 for one real probe:
+/* Regularizer term of traceEstimation.m:85-102 for one real probe:
  * tr = sum_w ||sqrt(We_w) .* IDFT3(conj(S_w) .* DFT3(probe))||^2 (host). */
 int disorder_shearlet_trace(disorder_ctx ctx, disorder_shearlet sh, const float* probe, const float* We,
                             double* tr);
-/* A probe of traceEstimation.m:34-38 on the device: V standard normals that
+/* A probe of traceEstimation.m:54-59 on the device: V standard normals that
  * depend only on (seed, index) (plugNoise(x,1)), scaled to unit mean square,
  * times mask (C.Ma, device real V) when given. probe: device V floats. */
 int disorder_trace_probe(disorder_ctx ctx, int64_t V, uint64_t seed, const float* mask, float* probe);
-/* Fidelity term of traceEstimation.m:40-61 for one real probe:
+/* Fidelity term of traceEstimation.m:61-84 for one real probe:
  * tr = sum_c sum_k W(k1,k2) |F2(S_c .* probe)(k)|^2, F2 the unitary DFT over
  * dims 1-2 (fftGPU/sqrt(N)); W: device N1 x N2 weights (EH.We on the grid).
  * Sf: device V x C complex. N1 and N2 as for shearlet_create. */

@@ -6,8 +6,8 @@ single precision):
 - Shearlets/getShearletIdxs.m:1-74 (without the name/value filters);
 - Shearlets/buildDirectionalFilter.m:25-47,149 ('ko' and 'kos');
 - Shearlets/buildQuadratureMirrorFilter.m ('maxflat2');
-- Shearlets/checkFilterFeasibility.m:1-28 (configuration 1 only);
-- Shearlets/buildWedgeBandpassAndLowpassFilters.m:1-71 (complex=0);
+- Shearlets/checkFilterFeasibility.m:1-38 (configuration 1 only);
+- Shearlets/buildWedgeBandpassAndLowpassFilters.m:1-129 (complex=0);
 - Methods/mirrorModulation.m, Methods/upsampling.m, Methods/shearing.m and
   Methods/resampling.m with fo=2 (centred crop / zero pad, no DFT);
 - the shearlet branch of Reconstruction/regularize.m:27-46, computeShearlet
@@ -42,7 +42,7 @@ def _as2d(v):
 
 
 def mirror_modulation(x, dirs=None):
-    """Methods/mirrorModulation.m:24-36 (c = 0): multiply by (-1)^n along the
+    """Methods/mirrorModulation.m:13-24 (c = 0): multiply by (-1)^n along the
     given dims (1-based), n the index relative to floor(N/2)+1."""
     x = np.array(_as2d(x), dtype=np.float64)
     N = _msize(x)
@@ -57,7 +57,7 @@ def mirror_modulation(x, dirs=None):
 
 
 def upsampling(x, dims, ups=2, odd=1):
-    """Methods/upsampling.m:18-33: insert ups-1 zeros between samples along
+    """Methods/upsampling.m:14-25: insert ups-1 zeros between samples along
     each dim (1-based); the new length is ups*N-(ups-1)*odd."""
     x = np.asarray(x)
     for d in ([dims] if np.isscalar(dims) else dims):
@@ -100,7 +100,7 @@ def resampling_space(x, Nres):
 
 
 def shearing_21(x, k):
-    """Methods/shearing.m:16-26 with dims = [2 1]: row n1 of x is shifted
+    """Methods/shearing.m:13-19 with dims = [2 1]: row n1 of x is shifted
     along dim 2 by -k*(n1 - floor(N1/2) - 1), through the DFT phase ramp of
     Methods/shifting.m:38-47 (the shift is an array, so the DFT branch)."""
     if k == 0:
@@ -122,14 +122,14 @@ def _conv2_col(a, col):
 
 
 def _fft2d(x):
-    """buildWedgeBandpassAndLowpassFilters.m:65-67: ifftshift then DFT, dims 1, 2."""
+    """buildWedgeBandpassAndLowpassFilters.m:121-123: ifftshift then DFT, dims 1, 2."""
     for m in (0, 1):
         x = fftGPU(np.fft.ifftshift(x, axes=m), m)
     return x
 
 
 def _ifft2d(x):
-    """buildWedgeBandpassAndLowpassFilters.m:69-71: inverse DFT then fftshift."""
+    """buildWedgeBandpassAndLowpassFilters.m:125-127: inverse DFT then fftshift."""
     for m in (0, 1):
         x = np.fft.fftshift(ifftGPU(x, m), axes=m)
     return x
@@ -161,7 +161,7 @@ _MAXFLAT2 = (.0104933261758410, -.0263483047033631, -.0517766952966370, .2763483
 
 def qmf_filter(QMFtype="maxflat2"):
     """Shearlets/buildQuadratureMirrorFilter.m: the 1-D scaling filter,
-    normalised to unit sum (:61)."""
+    normalised to unit sum (:60)."""
     if QMFtype != "maxflat2":
         raise NotImplementedError("quadrature mirror filter %s" % QMFtype)
     f = np.array(_MAXFLAT2, dtype=np.float64)
@@ -169,7 +169,7 @@ def qmf_filter(QMFtype="maxflat2"):
 
 
 def check_filter_feasibility(N, K, DF, SF):
-    """Shearlets/checkFilterFeasibility.m:4-28 for configuration 1 (the
+    """Shearlets/checkFilterFeasibility.m:16-38 for configuration 1 (the
     requested filters). Returns (DF, SF, WF, SF2)."""
     WF = mirror_modulation(SF)
     SF2 = SF
@@ -188,7 +188,7 @@ def check_filter_feasibility(N, K, DF, SF):
 
 
 def wedge_bandpass_lowpass(N, K, DF, SF1, WF, SF2):
-    """Shearlets/buildWedgeBandpassAndLowpassFilters.m:4-63 (complex = 0).
+    """Shearlets/buildWedgeBandpassAndLowpassFilters.m:34-119 (complex = 0).
     Returns (WD, BP, LP): WD[k] the (N1, N2, 2^(k+1)+1) wedge filters of
     shear level k (dict), BP (N1, N2, J) the bandpass filters, LP the lowpass,
     all in the frequency domain with frequency 0 first."""
@@ -202,16 +202,16 @@ def wedge_bandpass_lowpass(N, K, DF, SF1, WF, SF2):
     FHP[J - 1] = _as2d(WF)
     FLP1[J - 1] = _as2d(SF1)
     FLP2[Kmax - 1] = _as2d(SF2)
-    for j in range(J - 2, -1, -1):  # :24-27
+    for j in range(J - 2, -1, -1):  # :47-50
         FLP1[j] = _as2d(np.convolve(FLP1[J - 1].ravel(), upsampling(FLP1[j + 1], 2).ravel()))
         FHP[j] = _as2d(np.convolve(FLP1[J - 1].ravel(), upsampling(FHP[j + 1], 2).ravel()))
-    for k in range(Kmax - 2, -1, -1):  # :28-30
+    for k in range(Kmax - 2, -1, -1):  # :51-53
         FLP2[k] = _as2d(np.convolve(FLP2[Kmax - 1].ravel(), upsampling(FLP2[k + 1], 2).ravel()))
     BP = np.zeros(N + [J], dtype=np.complex128)
-    for j in range(J):  # :32-33
+    for j in range(J):  # :56-57
         BP[:, :, j] = _fft2d(resampling_space(FHP[j], N).astype(np.complex128))
     WD = {}
-    for k in sorted(set(K)):  # :43-61
+    for k in sorted(set(K)):  # :72-116
         WD[k] = np.zeros(N + [2 ** (k + 1) + 1], dtype=np.complex128)
         DFups = upsampling(DF, 1, 2 ** (k + 1))
         col = FLP2[Kmax - k - 1].ravel()
@@ -226,13 +226,13 @@ def wedge_bandpass_lowpass(N, K, DF, SF1, WF, SF2):
                 sh = _ifft2d(_fft2d(sh) * _fft2d(FLPauxfl))
             sh = (2 ** k) * sh[:, 0:(2 ** k) * N[1]:2 ** k]
             WD[k][:, :, 2 ** k - l] = _fft2d(sh)
-    LP = _fft2d(resampling_space(FLP1[0].T @ FLP1[0], N).astype(np.complex128))  # :63
+    LP = _fft2d(resampling_space(FLP1[0].T @ FLP1[0], N).astype(np.complex128))  # :119
     return WD, BP, LP
 
 
 # ---------------------------------------------------------------- the system
 def shearlet_idxs(ND, K, full=0):
-    """Shearlets/getShearletIdxs.m:27-52 (complex = 0, every scale, shearing,
+    """Shearlets/getShearletIdxs.m:29-74 (complex = 0, every scale, shearing,
     cone and pyramid): rows [cone scale half shearing] (2-D) or [pyramid
     scale half shearing1 shearing2] (3-D), 1-based, the lowpass row last."""
     rows = []
@@ -378,7 +378,7 @@ def regularize_sh(x, S, We, la, p=1.0):
 
 
 def _we_grid(E, EH):
-    """traceEstimation.m:24-29: the per-sample weights EH.We on the (ky, kz)
+    """traceEstimation.m:42-49: the per-sample weights EH.We on the (ky, kz)
     grid. Grid points that no sample hits get weight 0 (the reference leaves
     the entries that iSt does not overwrite as they were, which matters only
     when the samples do not cover the grid)."""
@@ -400,11 +400,11 @@ def trace_estimation(x, E=None, EH=None, C=None, R=None, tol=1e-2, BlSz=1, noise
         tr_round = []
         for _ in range(BlSz):
             v = np.asarray(noise(NX), np.float64)
-            v = v / np.sqrt(np.sum(v * v) / N)  # :35
+            v = v / np.sqrt(np.sum(v * v) / N)  # :55
             if C is not None and C.has("Ma"):
                 v = v * C.Ma
             tc = 0.0
-            if E is not None:  # :40-61
+            if E is not None:  # :61-84
                 xs = v[..., None] * np.asarray(E.Sf, np.complex128)
                 if W is not None:
                     for m in (0, 1):
@@ -412,7 +412,7 @@ def trace_estimation(x, E=None, EH=None, C=None, R=None, tol=1e-2, BlSz=1, noise
                     tc += float(np.sum(W[:, :, None, None] * np.abs(xs) ** 2))
                 else:
                     tc += float(np.sum(np.abs(xs) ** 2))
-            if R is not None and R.has("Sh"):  # :62-80
+            if R is not None and R.has("Sh"):  # :85-102
                 S, We = R.Sh.S, R.Sh.We
                 xF = _fft3(v.astype(np.complex128))
                 for w in range(S.shape[-1]):
@@ -423,5 +423,5 @@ def trace_estimation(x, E=None, EH=None, C=None, R=None, tol=1e-2, BlSz=1, noise
         n = len(trF)
         mea = float(np.mean(trF))
         std = float(np.std(trF, ddof=1)) / np.sqrt(n) if n > 1 else np.inf
-        if n >= 2 and std / (mea + EPS) < tol:  # :88-93
+        if n >= 2 and std / (mea + EPS) < tol:  # :106-112
             return mea, np.array(trF)

@@ -140,7 +140,7 @@ def test_device_probes(env):
         ctx.check(ctx.lib.disorder_trace_probe(ctx.h, V, 1234, None, d.ptr))
     pa, pb = a.numpy(), b.numpy()
     assert np.array_equal(pa, pb)  # a function of (seed, index) only
-    assert abs(np.mean(pa.astype(np.float64) ** 2) - 1) < 1e-5  # traceEstimation.m:35
+    assert abs(np.mean(pa.astype(np.float64) ** 2) - 1) < 1e-5  # traceEstimation.m:55
     assert abs(np.mean(pa)) < 0.02 and 0.9 < np.std(pa) < 1.1
     mask = (np.random.default_rng(9).uniform(size=N) > 0.5).astype(np.float32)
     ctx.check(ctx.lib.disorder_trace_probe(ctx.h, V, 1234, ctx.upload(mask).ptr, b.ptr))

@@ -136,7 +136,7 @@ def test_oracle_cs_beats_cg_at_scanner_intensities():
 
 def test_two_scale_planes_agree():
     """Two scales with shear levels 1 and 2 (the recursion of the lowpass and
-    highpass filters, buildWedgeBandpassAndLowpassFilters.m:24-30, and two
+    highpass filters, buildWedgeBandpassAndLowpassFilters.m:47-53, and two
     wedge sets) give the same 2-D planes from the device-form builder and the
     oracle."""
     Nt = (80, 76, 74)
