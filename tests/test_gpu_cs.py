@@ -155,11 +155,13 @@ def test_device_probes(env):
     assert abs(t_dev / t_host - 1) < 0.03
 
 
-@pytest.mark.parametrize("Nf", [(64, 64, 44), (64, 96, 88)])
+@pytest.mark.parametrize("Nf", [(64, 64, 44), (64, 96, 88), (256, 36, 40), (40, 176, 36), (36, 40, 128)])
 def test_register_fft_passes(Nf):
-    """Lengths with a fast factorisation take the register-FFT pass kernel
-    (64 = 8 x 8, 44 = 4 x 11, 96 = 8 x 12, 88 = 8 x 11; the
-    generic kernel covers the 40 and 36 of the other tests)."""
+    """Lengths with a fast factorisation take the register-FFT pass kernel:
+    64 = 8 x 8, 44 = 4 x 11, 88 = 8 x 11 (shearlet_fb.cu) and 256 = 16 x 16,
+    176 = 16 x 11, 128 = 16 x 8 (shearlet_fa.cu, the benchmark's lengths),
+    each on the contiguous axis or a strided one; 96, 40 and 36 take the
+    generic kernel."""
     import disorder_b200 as db
     from disorder_b200 import cs
     from oracle import shearlet as osh
