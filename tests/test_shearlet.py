@@ -147,3 +147,24 @@ def test_two_scale_planes_agree():
     for P, Q in zip(d_planes, o_planes):
         assert P.shape == Q.shape
         assert np.linalg.norm(P - Q) / np.linalg.norm(Q) < 1e-6
+
+
+def test_integer_shears_are_circular_row_shifts():
+    """Methods/shearing.m shears by a DFT phase ramp (shifting.m's array
+    branch); with integer shifts that is exactly a circular shift of each row,
+    which the device-form builder uses."""
+    rng = np.random.default_rng(13)
+    for shape in ((9, 17), (10, 16), (33, 65)):
+        v = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        for k in (-2, -1, 1, 2):
+            a = sh._shear_rows(v, k)
+            b = osh.shearing_21(v, k)
+            assert np.allclose(a, b, rtol=0, atol=1e-12 * np.abs(v).max()), (shape, k)
+
+
+def test_centred_crop_and_pad_agree():
+    """resampling.m with fo = 2 (centred zero pad or crop) in both builders."""
+    rng = np.random.default_rng(14)
+    for src, dst in (((1, 9), (40, 36)), ((33, 4), (40, 36)), ((9, 9), (36, 41)), ((41, 40), (36, 33))):
+        v = rng.standard_normal(src)
+        assert np.array_equal(sh._centre(v, dst), osh.resampling_space(v, dst))
