@@ -176,11 +176,10 @@ int dis_line_pass(disorder_ctx_s* ctx, LinePassArgs a) {
   a.L = pick_L(n, nbuf, 0);
   a.pitch = a.L + 1;
   const size_t smem = (size_t)((n + 1) & ~1) * sizeof(float2) + (size_t)nbuf * n * a.pitch * sizeof(float2);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(line_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  // set once per process (thread-safe static initialisation)
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(line_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  (void)attr;
   if (smem > 200 * 1024) return dis_set_error(ctx, DISORDER_BAD_ARG, "line pass: size %d too large", n);
   dim3 grid((unsigned)tiles_for(a.N, a.axis, a.L), a.accumulate ? 1 : (unsigned)a.n_slots);
   if (grid.x == 0 || grid.y == 0) return DISORDER_OK;
@@ -288,11 +287,9 @@ int dis_flip_pass(disorder_ctx_s* ctx, const disorder_plan_s* plan, float2* vols
   a.h2 = cent - 0.5f;
   a.plan = plan->fft[axis];
   const size_t smem = (size_t)((n + 1) & ~1) * sizeof(float2) + 2 * (size_t)n * a.pitch * sizeof(float2);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(flip_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(flip_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  (void)attr;
   dim3 grid((unsigned)tiles_for(plan->N, axis, a.L), (unsigned)n_slots);
   flip_kernel<<<grid, kThreads, smem, ctx->stream>>>(a);
   dis_count(ctx);

@@ -263,11 +263,10 @@ int dis_resample_axis(disorder_ctx_s* ctx, const float2* in, const int* Din, int
   a.in_vs = in_vs;
   a.out_vs = out_vs;
   const size_t smem = sizeof(float2) * (((nin + 1) & ~1) + ((nout + 1) & ~1) + 3 * (size_t)nmax * a.pitch);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(resample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  // set once per process (thread-safe static initialisation)
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(resample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  (void)attr;
   const int o1 = axis == 0 ? 1 : 0, o2 = axis == 2 ? 1 : 2;
   const long long nl = (long long)Din[o1] * Din[o2];
   dim3 grid((unsigned)((nl + L - 1) / L), (unsigned)nvol);

@@ -137,11 +137,11 @@ int sh_pass(disorder_ctx_s* ctx, ShArgs a) {
   while (a.L > 2 && (size_t)2 * n * (a.L + 1) * sizeof(float2) > 100 * 1024) a.L >>= 1;
   a.P = a.L + 1;
   const size_t smem = (size_t)((n + 1) & ~1) * sizeof(float2) + (size_t)2 * n * a.P * sizeof(float2);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(sh_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  // set once per process; the static's initialisation is thread-safe (host
+  // threads of several contexts launch concurrently)
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(sh_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  (void)attr;
   if (smem > 200 * 1024) return dis_set_error(ctx, DISORDER_UNSUPPORTED_FIELD, "shearlet: length %d too large", n);
   const size_t grid = tiles_for(a.N, a.axis, a.L);
   if (grid == 0) return DISORDER_OK;

@@ -250,11 +250,10 @@ bool sh_fast_launch_kind(disorder_ctx_s* ctx, const ShArgs& a) {
   using LN = ff::Line<F1, F2>;
   constexpr int N = LN::N, LPB = kThr / LN::TL;
   const size_t smem = sizeof(float2) * (((N + 1) & ~1) + ((LN::TWS + 1) & ~1) + (size_t)LPB * LN::EXSZ);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(sh_fast_kernel<F1, F2, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  // set once per process (thread-safe static initialisation)
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(sh_fast_kernel<F1, F2, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  (void)attr;
   const long long tiles = a.axis == 0 ? ((long long)a.N[1] * a.N[2] + LPB - 1) / LPB
                                       : (long long)((a.N[0] + LPB - 1) / LPB) * (a.axis == 1 ? a.N[2] : a.N[1]);
   if (tiles <= 0 || tiles >= (1LL << 31)) return false;
