@@ -1075,7 +1075,7 @@ def main():
         for name, lrn, prec in (("learned", True, "fp32"), ("mixed", False, "bf16x3")):
             variants[name] = variant_arm(ctx, sc, cfg, plain["ms"] * 1e-3, err, learned=lrn, precision=prec)
 
-    # roofline of the north star's unit, the normal operator (encodedecode) at
+    # roofline of the path's unit of work, the normal operator (encodedecode) at
     # full size, on its algorithmic bytes; the transform's line passes beside it
     peak, pkind = peaks()
     roof = normal_operator_roofline(ctx, cfg, peak, pkind)

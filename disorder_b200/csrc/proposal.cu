@@ -3,8 +3,8 @@
 // update, with its forward, backward and Adam kernels, plus the per-state
 // residual entry points it is fed by and the per-sample residual energies of
 // the driver's outlier weighting. There is no counterpart in the
-// reference; the plain Levenberg-Marquardt step (LMsolver.m) stays the judge
-// of every proposal (the caller accepts a proposal only where the state's
+// reference; the plain Levenberg-Marquardt step (LMsolver.m) still decides
+// on every proposal (the caller accepts a proposal only where the state's
 // energy drops).
 //
 // Activations are channels-last, level l holding [batch][n3][n2][n1][channel]

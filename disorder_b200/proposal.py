@@ -4,7 +4,7 @@ A small 3-D convolutional network, run and trained by the library's own
 kernels (``disorder_net_*`` in include/disorder.h), proposes each motion
 state's update from that state's back-projected k-space residual at the
 coarsest pyramid level. The plain Levenberg-Marquardt step
-(Reconstruction/LMsolver.m) stays the judge: ``propose_step`` keeps a
+(Reconstruction/LMsolver.m) still decides: ``propose_step`` keeps a
 proposal only for the states whose energy it lowers (the energy LMsolver.m
 evaluates at :82-83 and :196), and the LM step then runs from the kept
 motion, so a poor proposal costs at most the evaluation.

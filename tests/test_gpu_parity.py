@@ -1,7 +1,7 @@
 """GPU parity of libdisorder (through the C ABI) against the FP64 CPU oracle.
 
 Tolerance: the FP32 path must match the FP64 oracle to 1e-5 relative L2
-error on the transform and encoded k-space (the north-star FP32 bar); solver
+error on the transform and encoded k-space (the FP32 bar); solver
 outputs after several iterations use 1e-4 (iteration amplifies rounding).
 """
 
