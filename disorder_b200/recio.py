@@ -14,10 +14,11 @@ Conventions follow solveXT.m: the phase encodes are permuted to the first
 dimensions with perm(1:3) = [3 2 1] (:51), so grid dimension 1 is the
 scanner's dimension 3 and grid dimension 2 its dimension 2 (:80, :99).
 
-Not restated here (the rest of solveXT.m's ingestion of the ``rec``
-structure): the readout ROI (computeROI / extractROI, :40-47), the Tukey
-apodization (buildFilter, :70) and reading ``rec`` files, which writeRaw.m
-saves as MATLAB v7.3 (HDF5) files.
+``prepare_rec`` is the data steps before it (solveXT.m:39-72): the readout
+ROI (computeROI / extractROI), the permutation of the phase encodes to the
+front, the Tukey apodization (buildFilter 'tukey') and the averages folded
+into dimension 5 (resSub). Not restated: reading ``rec`` files, which
+writeRaw.m saves as MATLAB v7.3 (HDF5) files.
 """
 
 import math
@@ -127,3 +128,118 @@ def profile_order(Shot, Echo, N, shots=None):
     k2 = np.broadcast_to(c[1][None, :], N)[sel]
     order = np.lexsort((Echo[sel], Shot[sel]))
     return k2[order], k1[order]  # z{2} is grid dim 2, z{3} grid dim 1
+
+
+# ---------------------------------------------------------------- data preparation
+def compute_roi(x, ext=0, sy=None, ev=None, fu=0):
+    """Methods/computeROI.m:20-57: the bounding box of |x| > 1e-6 per
+    dimension (the first 3 unless fu), widened by ext, optionally made
+    symmetric (sy) or of even extent (ev). Rows [first last N extent before
+    after], 1-based like the reference."""
+    a = np.abs(np.asarray(x)) > 1e-6
+    ND = a.ndim if fu else min(a.ndim, 3)
+    sy = np.zeros(ND) if sy is None else np.asarray(sy)
+    ev = np.zeros(ND) if ev is None else np.asarray(ev)
+    if not a.any():
+        raise ValueError("computeROI: the array has no element above 1e-6")
+    ROI = np.zeros((ND, 6), np.int64)
+    for n in range(ND):
+        other = tuple(d for d in range(a.ndim) if d != n)
+        hit = np.flatnonzero(a.any(axis=other))
+        ROI[n, :3] = (hit[0] + 1, hit[-1] + 1, a.shape[n])
+    ROI[:, 0] = np.maximum(ROI[:, 0] - ext, 1)
+    ROI[:, 1] = np.minimum(ROI[:, 1] + ext, ROI[:, 2])
+    ROI[:, 3] = ROI[:, 1] - ROI[:, 0] + 1
+    ROI[:, 4] = ROI[:, 0] - 1
+    ROI[:, 5] = ROI[:, 2] - ROI[:, 1]
+    for n in range(ND):
+        if sy[n]:
+            d = ROI[n, 5] - ROI[n, 4]
+            ROI[n, [1 if ROI[n, 4] <= ROI[n, 5] else 0, 3]] += d  # the side with the smaller margin
+            ROI[n, 5] = ROI[n, 4]
+        if ev[n] and ROI[n, 3] % 2:
+            ROI[n, 3] -= 1
+            ROI[n, [0, 4]] += 1
+    return ROI
+
+
+def extract_roi(x, ROI, ext=1, dims=None):
+    """Methods/extractROI.m:14-28: crop x to ROI rows first:last along dims
+    (ext = 1), or place x there in zeros of the full size (ext = 0)."""
+    x = np.asarray(x)
+    ND = min(ROI.shape[0], x.ndim)
+    dims = list(range(1, ND + 1)) if dims is None else ([dims] if np.isscalar(dims) else list(dims))
+    sl = [slice(None)] * x.ndim
+    for d in dims:
+        sl[d - 1] = slice(int(ROI[d - 1, 0]) - 1, int(ROI[d - 1, 1]))
+    if ext:
+        return x[tuple(sl)]
+    shape = list(x.shape)
+    for d in dims:
+        shape[d - 1] = int(ROI[d - 1, 2])
+    y = np.zeros(shape, dtype=x.dtype)
+    y[tuple(sl)] = x
+    return y
+
+
+def tukey_filter(N, sp, gibbsRing):
+    """Methods/buildFilter.m:93-101 ('tukey', c = 0): the product over dims
+    of 1-D Tukey windows of the radial k of each dim,
+    k = 2 pi |n - ceil((N+1)/2)| / (sp N) (generateGrid with nor 2 i pi / sp,
+    :29), 1 below pi (1 - g), a raised cosine up to pi, 0 beyond
+    (tukeyIso, :86-92); then fftshift."""
+    N = [int(n) for n in N]
+    ND = len(N)
+    sp = np.broadcast_to(np.asarray(sp, np.float64), (ND,))
+    g = list(np.atleast_1d(np.asarray(gibbsRing, np.float64)))
+    g = g + [g[-1]] * (ND - len(g))
+    x = np.ones(N)
+    for m in range(ND):
+        n = np.arange(1, N[m] + 1)
+        kk = np.abs(2 * np.pi / sp[m] / N[m] * (n - math.ceil((N[m] + 1) / 2)))
+        w = np.ones(N[m])
+        alpha = 1 - g[m]
+        if g[m] != 0:
+            taper = kk >= np.pi * alpha
+            w[taper] = 0.5 * (1 + np.cos(np.pi * ((kk[taper] - np.pi * alpha) / ((1 - alpha) * np.pi))))
+        w[kk >= np.pi] = 0
+        shape = [1] * ND
+        shape[m] = N[m]
+        x = x * w.reshape(shape)
+    return np.fft.fftshift(x)
+
+
+def merge_averages(y, first=5):
+    """Methods/resSub.m:15-30 with orDim = first:ndims: the dimensions from
+    `first` (1-based) on folded into one."""
+    y = np.asarray(y)
+    if y.ndim < first:
+        return y
+    return y.reshape(y.shape[:first - 1] + (int(np.prod(y.shape[first - 1:])),), order="F")
+
+
+def prepare_rec(y, S, M, voxSiz, apod=(0.1, 0.0, 0.0)):
+    """The data steps of solveXT.m:39-72 in their order: the readout ROI of
+    the mask with even extent (computeROI(rec.M,[],[0 0 0],[1 0 0]), :40),
+    y, S and M cropped to it along dim 1 (extractROI(.,ROI,1,1), :45-47),
+    the phase encodes permuted to the front (perm(1:3) = [3 2 1], :50-57),
+    the Tukey apodization of y (buildFilter(NY(1:3),'tukey',[10 10 1],gpu,
+    apod) ifftshifted, :70) and the averages folded into dim 5 (resSub,
+    :71). Returns a dict with y, S, M, ROI, voxSiz and NY (the size of y
+    with the averages as dim 5)."""
+    M = np.asarray(M)
+    ROI = compute_roi(M, 0, [0, 0, 0], [1, 0, 0])
+    y = extract_roi(y, ROI, 1, 1)
+    S = extract_roi(S, ROI, 1, 1)
+    M = extract_roi(M, ROI, 1, 1)
+    perm = lambda a: np.transpose(a, (2, 1, 0) + tuple(range(3, np.ndim(a))))  # noqa: E731
+    y, S, M = perm(y), perm(S), perm(M)
+    voxSiz = tuple(np.asarray(voxSiz, np.float64)[[2, 1, 0]])
+    ap = np.asarray(apod, np.float64)[[2, 1, 0]]
+    NY = y.shape
+    w = np.fft.ifftshift(tukey_filter(NY[:3], [10, 10, 1], ap)).astype(np.float32 if y.dtype == np.complex64
+                                                                     else np.float64)
+    y = y * w.reshape(NY[:3] + (1,) * (y.ndim - 3))
+    y = merge_averages(y, 5)
+    NYo = tuple(y.shape) + (1,) * (5 - y.ndim)
+    return {"y": y, "S": S, "M": M, "ROI": ROI, "voxSiz": voxSiz, "NY": NYo}

@@ -1,8 +1,10 @@
 """Acquisition structure of Reconstruction/solveXT.m (oracle).
 
 TEST INFRASTRUCTURE ONLY. Restates solveXT.m:74-142 loop by loop (the
-profile -> shot / sweep assignment and the timeIndex fill) and Methods/fct.m
-(the orthonormal DCT-II by Makhoul's reordering and one FFT), in float64.
+profile -> shot / sweep assignment and the timeIndex fill), Methods/fct.m
+(the orthonormal DCT-II by Makhoul's reordering and one FFT), and the data
+steps of solveXT.m:39-72 (Methods/computeROI.m, extractROI.m, the 'tukey'
+filter of buildFilter.m and resSub.m), in float64.
 """
 
 import math
@@ -90,3 +92,101 @@ def acquisition_structure(z2, z3, kRange2, kRange3, TFEfactor, ZReconLength=1, N
     return {"NEchos": NEchos, "NShots": NShots, "NProfs": NProfs, "NSweeps": NSweeps, "steady_state": steady,
             "kTraj": np.array(kTraj), "kShift": np.array(kShift, float), "kSize": np.array(kSize, float),
             "kIndex": np.array(kIndex), "sweepSample": np.array(sweepSample), "timeIndex": timeIndex, "H": H}
+
+
+def computeROI(x, ext=0, sy=None, ev=None, fu=0):
+    """Methods/computeROI.m:20-57, the while loops as written."""
+    a = (np.abs(np.asarray(x)) > 1e-6).astype(np.float64)
+    ND = a.ndim if fu else min(a.ndim, 3)
+    sy = [0] * ND if sy is None else list(sy)
+    ev = [0] * ND if ev is None else list(ev)
+    ROI = np.zeros((ND, 6))
+    for n in range(ND):
+        ROI[n, 0], ROI[n, 1], ROI[n, 2] = 1, a.shape[n], a.shape[n]
+    step = [1, -1]
+    for l in range(2):
+        for n in range(ND):
+            while not np.any(np.take(a, int(ROI[n, l]) - 1, axis=n)):
+                ROI[n, l] += step[l]
+    ROI[:, 0] = np.maximum(ROI[:, 0] - ext, 1)
+    ROI[:, 1] = np.minimum(ROI[:, 1] + ext, ROI[:, 2])
+    ROI[:, 3] = ROI[:, 1] - ROI[:, 0] + 1
+    ROI[:, 4] = ROI[:, 0] - 1
+    ROI[:, 5] = ROI[:, 2] - ROI[:, 1]
+    for n in range(ND):
+        if sy[n]:
+            indSm = 1 if ROI[n, 4] <= ROI[n, 5] else 2
+            for col in (3 - indSm, 4):
+                ROI[n, col - 1] += ROI[n, 5] - ROI[n, 4]
+            ROI[n, 5] = ROI[n, 4]
+        if ev[n] and ROI[n, 3] % 2 != 0:
+            ROI[n, 3] -= 1
+            ROI[n, 0] += 1
+            ROI[n, 4] += 1
+    return ROI.astype(np.int64)
+
+
+def extractROI(x, ROI, ext=1, dims=None):
+    """Methods/extractROI.m:14-28."""
+    x = np.asarray(x)
+    ND = min(ROI.shape[0], x.ndim)
+    dims = list(range(1, ND + 1)) if dims is None else ([dims] if np.isscalar(dims) else list(dims))
+    idx = [np.arange(x.shape[d]) for d in range(x.ndim)]
+    for d in dims:
+        idx[d - 1] = np.arange(int(ROI[d - 1, 0]) - 1, int(ROI[d - 1, 1]))
+    if ext:
+        return x[np.ix_(*idx)]
+    shape = list(x.shape)
+    for d in dims:
+        shape[d - 1] = int(ROI[d - 1, 2])
+    y = np.zeros(shape, dtype=x.dtype)
+    y[np.ix_(*idx)] = x
+    return y
+
+
+def buildFilter_tukey(N, sp, gibbsRing):
+    """Methods/buildFilter.m:93-101 ('tukey') with the 1-D 'tukeyIso' windows
+    of :69-92, element by element."""
+    ND = len(N)
+    sp = list(np.broadcast_to(np.asarray(sp, np.float64), (ND,)))
+    g = list(np.atleast_1d(np.asarray(gibbsRing, np.float64)))
+    g = g + [g[-1]] * (ND - len(g))
+    x = np.ones(N)
+    for m in range(ND):
+        cent = math.ceil((N[m] + 1) / 2)
+        w = np.ones(N[m])
+        alpha = 1 - g[m]
+        for i in range(N[m]):
+            kk = abs((2 * np.pi / sp[m]) / N[m] * ((i + 1) - cent))
+            if g[m] != 0 and kk >= np.pi * alpha:
+                w[i] = 0.5 * (1 + math.cos(math.pi * ((kk - math.pi * alpha) / ((1 - alpha) * math.pi))))
+            if kk >= np.pi:
+                w[i] = 0
+        shape = [1] * ND
+        shape[m] = N[m]
+        x = x * w.reshape(shape)
+    return np.fft.fftshift(x)
+
+
+def resSub(x, first=5):
+    """Methods/resSub.m:15-30 with orDim = first:ndims(x)."""
+    x = np.asarray(x)
+    if x.ndim < first:
+        return x
+    N = list(x.shape[:first - 1]) + [int(np.prod(x.shape[first - 1:]))]
+    return x.reshape(N, order="F")
+
+
+def prepare_rec(y, S, M, voxSiz, apod=(0.1, 0.0, 0.0)):
+    """solveXT.m:39-72, the data steps in order."""
+    ROI = computeROI(M, 0, [0, 0, 0], [1, 0, 0])
+    y, S, M = (extractROI(a, ROI, 1, 1) for a in (y, S, M))
+    perm = lambda a: np.transpose(a, [2, 1, 0] + list(range(3, np.ndim(a))))  # noqa: E731
+    y, S, M = perm(y), perm(S), perm(M)
+    voxSiz = [voxSiz[2], voxSiz[1], voxSiz[0]]
+    ap = [apod[2], apod[1], apod[0]]
+    NY = y.shape
+    w = np.fft.ifftshift(buildFilter_tukey(list(NY[:3]), [10, 10, 1], ap))
+    y = y * w.reshape(tuple(NY[:3]) + (1,) * (y.ndim - 3))
+    y = resSub(y, 5)
+    return {"y": y, "S": S, "M": M, "ROI": ROI, "voxSiz": tuple(voxSiz)}

@@ -116,3 +116,55 @@ def test_disorder_trajectory_round_trip(order):
     _same(a, orec.acquisition_structure(z2, z3, r, r, TFEfactor=NP // 16))
     assert a["NShots"] == 16
     assert np.array_equal(a["H"], sampling.shot_map(Shot))
+
+
+def test_roi_against_the_while_loops():
+    rng = np.random.default_rng(5)
+    for _ in range(15):
+        M = np.zeros((int(rng.integers(9, 20)), int(rng.integers(5, 12)), int(rng.integers(4, 9))))
+        sl = tuple(slice(int(rng.integers(0, s // 2)), int(rng.integers(s // 2 + 1, s + 1))) for s in M.shape)
+        M[sl] = rng.uniform(0.5, 1.0)
+        for sy in ([0, 0, 0], [1, 0, 1]):
+            for ev in ([0, 0, 0], [1, 1, 1]):
+                for ext in (0, 2):
+                    assert np.array_equal(recio.compute_roi(M, ext, sy, ev), orec.computeROI(M, ext, sy, ev))
+        R = recio.compute_roi(M, 1, [0, 0, 0], [1, 0, 0])
+        for dims in (1, [1, 3], None):
+            crop = recio.extract_roi(M, R, 1, dims)  # ext = 1 crops, ext = 0 puts back
+            assert np.array_equal(crop, orec.extractROI(M, R, 1, dims))
+            back = recio.extract_roi(crop, R, 0, dims)
+            assert np.array_equal(back, orec.extractROI(crop, R, 0, dims))
+            assert back.shape == M.shape and np.array_equal(back * (M != 0), M)
+    with pytest.raises(ValueError):
+        recio.compute_roi(np.zeros((4, 4, 4)))
+
+
+def test_tukey_window():
+    for N, sp, g in (((16,), [1], [0.5]), ((9, 12, 7), [10, 10, 1], [0.0, 0.0, 0.1]), ((20, 11, 8), [1, 2, 1], [0.3])):
+        a = recio.tukey_filter(N, sp, g)
+        b = orec.buildFilter_tukey(list(N), sp, g)
+        assert np.allclose(a, b, rtol=0, atol=1e-12)
+    # one dimension, no taper: 1 up to the band edge, 0 at k = pi (the most
+    # negative frequency of an even length), DC first after fftshift
+    w = np.fft.ifftshift(recio.tukey_filter((8,), [1], [0.0]))
+    assert w[0] == 0 and np.all(w[1:] == 1)
+    w = np.fft.ifftshift(recio.tukey_filter((8,), [1], [0.5]))
+    assert np.allclose(w, [0, 0.5, 1, 1, 1, 1, 1, 0.5])
+
+
+def test_prepare_rec_against_the_oracle():
+    rng = np.random.default_rng(6)
+    Nr, Ny, Nz, C = 24, 10, 8, 3
+    M = np.zeros((Nr, Ny, Nz))
+    M[5:18, 1:9, 2:7] = 1
+    y = (rng.standard_normal((Nr, Ny, Nz, C, 2, 2)) + 1j * rng.standard_normal((Nr, Ny, Nz, C, 2, 2)))
+    S = rng.standard_normal((Nr, Ny, Nz, C)) + 1j * rng.standard_normal((Nr, Ny, Nz, C))
+    a = recio.prepare_rec(y, S, M, (0.5, 1.0, 2.0), apod=(0.1, 0.0, 0.0))
+    b = orec.prepare_rec(y, S, M, (0.5, 1.0, 2.0), apod=(0.1, 0.0, 0.0))
+    # the readout ROI of the mask is 13 samples, evened to 12 (ev = [1 0 0])
+    assert list(a["ROI"][0, :4]) == [7, 18, 24, 12]
+    assert a["y"].shape == (Nz, Ny, 12, C, 4) and a["S"].shape == (Nz, Ny, 12, C) and a["M"].shape == (Nz, Ny, 12)
+    assert a["voxSiz"] == (2.0, 1.0, 0.5) and a["NY"] == (Nz, Ny, 12, C, 4)
+    for k in ("y", "S", "M"):
+        assert np.allclose(a[k], b[k], rtol=0, atol=1e-12)
+    assert np.array_equal(a["ROI"], b["ROI"])
